@@ -1,0 +1,368 @@
+#!/usr/bin/env python3
+"""Benchmark: patches/s per K-SVD iteration (OMP + dictionary update).
+
+Workload (default): one 2048 x 2048 synthetic grayscale image (seeded
+gratings + flat rectangles, Gaussian noise sigma 25), 12 x 12 patches at
+stride 3 (679^2 = 461,041 patches of 144 values), 256 atoms, OMP limited to
+5 atoms, 10 K-SVD iterations for the end-to-end call.
+
+A "step" is one K-SVD iteration over all patches (kSvd's loop body,
+cuda_svd_denoiser.cu:374-397).  value = patches x steps / device time of the
+steps (max over ranks), inputs resident in HBM.  The patch matrix (265 MB) is
+larger than L2, so no explicit flush is needed between steps.
+
+e2e = the same metric through the C ABI's ksvd_denoise with host buffers
+(pinned): H2D of the image, patch gather, dictionary init, all iterations,
+final OMP, image rebuild, D2H of the result, all inside the timed region;
+value = patches x iterations / time per call.
+
+Multi-GPU: the K-SVD iteration does not shard without a collective inside
+the sequential atom sweep, so N GPUs run N independent replicas (each rank
+its own seeded image): weak scaling, no data-path collective.
+
+--impl reference times the CPU restatement of the reference's algorithm
+(the reference has no CPU implementation of K-SVD) on the host cores.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+from ksvd_loader import load, load_oracle  # noqa: E402
+
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
+
+
+def read_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            d = json.loads(p.read_text())
+            return d, "measured"
+        except Exception:
+            pass
+    return PEAKS_FALLBACK, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def cpu_baseline(pkg, oracle, wl, budget_s=20.0, max_patches=None):
+    """One K-SVD iteration (OMP + update) of the CPU FP32 restatement on a
+    bounded contiguous sample of the workload's patches, all host threads."""
+    clean, noisy = wl.images()
+    Y = oracle.extract_patches(noisy, wl.patch, wl.patch, wl.stride, wl.stride)
+    N = Y.shape[0]
+    D = oracle.init_dictionary(Y, wl.atoms, int_norm=True, dtype=np.float32)
+    # calibrate on a small slice, then size the sample for the budget
+    n0 = min(N, 4096)
+    t = time.perf_counter()
+    idx, coef = oracle.omp(Y[:n0], D, wl.omp_iter, dtype=np.float32)
+    oracle.update_dictionary(Y[:n0], D, idx, coef, q1_cap=False, dtype=np.float32)
+    dt = time.perf_counter() - t
+    ns = int(min(N, max(n0, n0 * budget_s / max(dt, 1e-3) * 0.8)))
+    if max_patches:
+        ns = min(ns, max_patches)
+    start = (N - ns) // 2
+    Ys = np.ascontiguousarray(Y[start:start + ns])
+    t = time.perf_counter()
+    idx, coef = oracle.omp(Ys, D, wl.omp_iter, dtype=np.float32)
+    oracle.update_dictionary(Ys, D, idx, coef, q1_cap=False, dtype=np.float32)
+    dt = time.perf_counter() - t
+    return {"value": ns / dt, "unit": "patches/s", "cores": oracle.max_threads(), "kind": "port",
+            "sample": f"1 K-SVD iteration (FP32 OMP + full update sweep) on {ns} of the workload's {N} patches "
+                      f"(contiguous middle slice), {wl.atoms} atoms, L={wl.omp_iter}, {dt:.1f} s"}, dt
+
+
+def run_reference(args, wl):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    pkg = load()
+    oracle = load_oracle()
+    clean, noisy = wl.images()
+    Y = oracle.extract_patches(noisy, wl.patch, wl.patch, wl.stride, wl.stride)
+    N = Y.shape[0]
+    D0 = oracle.init_dictionary(Y, wl.atoms, int_norm=True, dtype=np.float32)
+    # size each step so that warmup + steps fit in about two minutes
+    n0 = min(N, 4096)
+    t = time.perf_counter()
+    idx, coef = oracle.omp(Y[:n0], D0, wl.omp_iter, dtype=np.float32)
+    oracle.update_dictionary(Y[:n0], D0, idx, coef, q1_cap=False, dtype=np.float32)
+    per_patch = (time.perf_counter() - t) / n0
+    steps_total = args.steps + args.warmup
+    ns = int(min(N, max(n0, 120.0 / steps_total / max(per_patch, 1e-9))))
+    start = (N - ns) // 2
+    Ys = np.ascontiguousarray(Y[start:start + ns])
+    D = D0.copy()
+    times = []
+    for i in range(steps_total):
+        t = time.perf_counter()
+        idx, coef = oracle.omp(Ys, D, wl.omp_iter, dtype=np.float32)
+        D, coef = oracle.update_dictionary(Ys, D, idx, coef, q1_cap=False, dtype=np.float32)
+        if i >= args.warmup:
+            times.append(time.perf_counter() - t)
+    ms = 1000.0 * float(np.mean(times))
+    value = ns / (ms / 1000.0)
+    cores = oracle.max_threads()
+    line = {
+        "metric": "patches/s per K-SVD iteration", "value": value, "unit": "patches/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": wl.name, "image": f"{wl.size}x{wl.size}", "sigma": wl.sigma,
+                   "patch": f"{wl.patch}x{wl.patch}", "stride": wl.stride, "num_patches": N, "atoms": wl.atoms,
+                   "omp_iter": wl.omp_iter, "sample_patches": ns},
+        "cpu_baseline": {"value": value, "unit": "patches/s", "cores": cores, "kind": "port",
+                         "sample": f"each step: 1 K-SVD iteration on {ns} of {N} patches (contiguous middle "
+                                   f"slice), FP32 CPU restatement, {cores} threads"},
+        "e2e": {"value": value, "unit": "patches/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="img2048_p12s3_k256")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16"])
+    ap.add_argument("--compat", type=int, default=1, help="KSVD_COMPAT_* bits (1 = INT_NORM, 3 = +Q1 cap)")
+    ap.add_argument("--e2e-calls", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    pkg = load()
+    wl = pkg.synth.WORKLOADS[args.workload]
+    if args.impl == "reference":
+        return run_reference(args, wl)
+
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+
+    ksvd = pkg.ksvd
+    prec = ksvd.PREC_FP32 if args.precision == "fp32" else ksvd.PREC_BF16_RESCORE
+    params = ksvd.make_params(patch_width_dim=wl.patch, patch_height_dim=wl.patch, sliding_width=wl.stride,
+                              sliding_height=wl.stride, atoms=wl.atoms, omp_iter=wl.omp_iter,
+                              ksvd_iter=wl.ksvd_iter, precision=prec, compat=args.compat, device=local)
+    ctx = ksvd.Context(params)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+
+    # each rank: its own seeded image (replicas)
+    from dataclasses import replace
+    wlr = replace(wl, seed=wl.seed + rank)
+    clean, noisy = wlr.images()
+    H, W = noisy.shape
+    N = ksvd.num_patches(params, W, H)
+    n, K, L = wl.n, wl.atoms, wl.omp_iter
+    sigma2 = wl.sigma ** 2
+
+    with torch.cuda.stream(stream):
+        img_d = torch.from_numpy(noisy).cuda()
+        patches = torch.empty((N, n), dtype=torch.float32, device="cuda")
+        D = torch.empty((K, n), dtype=torch.float32, device="cuda")
+        idx = torch.empty((N, L), dtype=torch.int32, device="cuda")
+        coef = torch.empty((N, L), dtype=torch.float32, device="cuda")
+    stream.synchronize()
+    ctx.extract_patches(img_d, patches)
+    ctx.init_dictionary(patches, D)
+    D0 = D.clone()
+    stream.synchronize()
+
+    # ---- warm-up, then K timed K-SVD iterations ---------------------------
+    for _ in range(args.warmup):
+        ctx.iterate(patches, D, idx, coef, 1)
+    stream.synchronize()
+    with torch.cuda.stream(stream):
+        D.copy_(D0)
+    ctx.profile(True)
+    ctx.profile_reset()
+    launches0 = ctx.launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            ctx.iterate(patches, D, idx, coef, 1)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms_total = ev0.elapsed_time(ev1)
+    gpu_launches = ctx.launch_count() - launches0
+    fam = {f: ctx.profile_read(f) for f in ("gram", "omp", "csr", "update")}
+    ctx.profile(False)
+    ms_step = ms_total / args.steps
+    if dist:
+        t = torch.tensor([ms_step], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_step = float(t.item())
+    value = N * world / (ms_step / 1000.0)
+
+    # ---- e2e through the C ABI with pinned host buffers --------------------
+    img_h = torch.from_numpy(noisy).pin_memory()
+    out_h = torch.empty_like(img_h).pin_memory()
+    e2e_ms = []
+    st = None
+    for i in range(args.e2e_calls + 1):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st = ctx.denoise_ptr(img_h.data_ptr(), W, H, sigma2, out_h.data_ptr())
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if i > 0:  # first call is a warm-up
+            e2e_ms.append(e0.elapsed_time(e1))
+    e2e_call_ms = float(np.median(e2e_ms))
+    if dist:
+        t = torch.tensor([e2e_call_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_call_ms = float(t.item())
+    e2e_value = N * wl.ksvd_iter * world / (e2e_call_ms / 1000.0)
+    out = out_h.numpy()
+    psnr_noisy = pkg.synth.psnr(clean, noisy)
+    psnr_out = pkg.synth.psnr(clean, out)
+
+    if rank == 0:
+        peaks, peak_src = read_peaks()
+        # dominant kernel by device time
+        dom = max(("omp", "update"), key=lambda f: fam[f][0])
+        dom_ms, dom_launches = fam[dom]
+        avg_ms = dom_ms / max(dom_launches, 1)
+        # algorithmic bytes per launch (per patch figures):
+        #   omp: read the patch (4n) + write the codes (8L)
+        #   update: read the patch once per used atom + code (L(4n+8)) + write coefficients (4L)
+        if dom == "omp":
+            bytes_per_patch = 4 * n + 8 * L
+        else:
+            bytes_per_patch = L * (4 * n + 8) + 4 * L
+        traffic_file = ROOT / "profiles" / f"traffic_{wl.name}_{args.precision}.json"
+        traffic = None
+        if traffic_file.exists():
+            try:
+                traffic = json.loads(traffic_file.read_text()).get(dom)
+            except Exception:
+                traffic = None
+        achieved = bytes_per_patch * N / (avg_ms / 1000.0) / 1e9
+        peak = float(peaks.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"]))
+        cpu = None
+        if not args.no_cpu_baseline:
+            oracle = load_oracle()
+            cpu, _ = cpu_baseline(pkg, oracle, wl, budget_s=args.cpu_budget)
+        line = {
+            "metric": "patches/s per K-SVD iteration", "value": value, "unit": "patches/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else "bf16+f32",
+            "data": "synthetic",
+            "config": {"workload": wl.name, "image": f"{wl.size}x{wl.size}", "sigma": wl.sigma,
+                       "patch": f"{wl.patch}x{wl.patch}", "stride": wl.stride, "num_patches": N, "atoms": K,
+                       "omp_iter": L, "precision": args.precision, "compat": args.compat,
+                       "l2": "inputs larger than L2 (265 MB patch matrix), no flush",
+                       "parallelism": f"replicas x{world}"},
+            "e2e": {"value": e2e_value, "unit": "patches/s", "h2d_bytes_per_step": int(W * H * 4),
+                    "d2h_bytes_per_step": int(W * H * 4), "ms_per_call": e2e_call_ms,
+                    "ksvd_iter_per_call": wl.ksvd_iter},
+            "gpu_launches": int(gpu_launches),
+            "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
+                         "algorithmic_bytes_per_patch": bytes_per_patch, "avg_launch_ms": avg_ms},
+            "kernel_ms_per_step": {f: fam[f][0] / max(args.steps, 1) for f in fam},
+            "quality": {"psnr_noisy": psnr_noisy, "psnr_denoised": psnr_out,
+                        "power_iters_last_sweep": st.power_iters, "atoms_updated_last_sweep": st.atoms_updated},
+            "clocks": clocks.summary(),
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,122 @@
+// Device helpers: warp reductions, acquire/release accesses, the bounded
+// software grid barrier of the persistent kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "ksvd_internal.cuh"
+
+namespace ksvd {
+
+#define KSVD_DEV __device__ __forceinline__
+
+// Wall-clock limit of one grid-barrier wait (ns).  A wait that runs this long
+// sets DEVERR_TIMEOUT and returns; every later wait sees the flag and returns
+// at once, so a failed launch ends within about this long.
+constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;
+
+KSVD_DEV unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+KSVD_DEV unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+KSVD_DEV void st_release_u32(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+KSVD_DEV int ld_relaxed_i32(const int* p) {
+  int v;
+  asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+template <typename T>
+KSVD_DEV T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+KSVD_DEV float warp_max(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Block-wide sum; `red` is shared scratch of at least 32 elements.  All
+// threads get the result.
+template <typename T>
+__device__ T block_sum(T v, T* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = (blockDim.x + 31) >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  T t = (threadIdx.x < nw) ? red[threadIdx.x] : T(0);
+  if (warp == 0) t = warp_sum(t);
+  if (threadIdx.x == 0) red[0] = t;
+  __syncthreads();
+  return red[0];
+}
+
+__device__ inline float block_max(float v, float* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = (blockDim.x + 31) >> 5;
+  v = warp_max(v);
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  float t = (threadIdx.x < nw) ? red[threadIdx.x] : 0.0f;
+  if (warp == 0) t = warp_max(t);
+  if (threadIdx.x == 0) red[0] = t;
+  __syncthreads();
+  return red[0];
+}
+
+// Software grid barrier for a cooperative launch (all CTAs co-resident).
+// Returns false when an error is flagged: this CTA's wait timed out, or
+// another CTA flagged one.  Every wait is bounded by kBarrierTimeoutNs.
+__device__ inline bool grid_sync(GridBarrier* b, unsigned nblocks) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    unsigned gen = ld_acquire_u32(&b->gen);
+    __threadfence();
+    unsigned arrived = atomicAdd(&b->count, 1u);
+    if (arrived == nblocks - 1) {
+      atomicExch(&b->count, 0u);
+      __threadfence();
+      st_release_u32(&b->gen, gen + 1u);
+    } else {
+      unsigned long long t0 = globaltimer_ns();
+      while (ld_acquire_u32(&b->gen) == gen) {
+        if (ld_relaxed_i32(&b->err) != DEVERR_NONE) {
+          ok = 0;
+          break;
+        }
+        if (globaltimer_ns() - t0 > kBarrierTimeoutNs) {
+          atomicCAS(&b->err, DEVERR_NONE, DEVERR_TIMEOUT);
+          ok = 0;
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    if (ok && ld_relaxed_i32(&b->err) != DEVERR_NONE) ok = 0;
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+}  // namespace ksvd

@@ -1,0 +1,312 @@
+// Batched OMP sparse coding, plain FP32 form (CuBlasMatrixOmp::work,
+// cublas_matrix_omp.cu:107-402).
+//
+// The reference runs each OMP step as one cuBLAS SGEMM (D^T R) followed by
+// about 4 N per-patch cuBLAS calls issued from host loops (Isamax, gesvda
+// pseudo-inverse, two Sgemv, Snrm2).  Here one persistent kernel does every
+// step of every patch on chip:
+//   * the CTA keeps the whole dictionary in shared memory, k-major, and walks
+//     tiles of kTP patches (grid = one CTA per SM);
+//   * per step, the K x kTP correlation D^T R is a register-tiled FP32 SIMT
+//     product (8 atoms x 4 patches per thread, 16-byte shared loads);
+//   * argmax |.| per patch with the lowest atom index winning ties, as
+//     cublasIsamax does (:216-233);
+//   * the least-squares coefficients on the support (the reference's
+//     pseudo-inverse, :269-339) come from a Cholesky factor of the support
+//     Gram grown by one row per step, in FP64 from the FP64 dictionary Gram;
+//   * the residual y - D_S g (:352-380) and its norm (:382-393) are formed
+//     per patch by one warp; a patch whose residual norm is below 1e-3 stops
+//     (:218).
+#include <cuda_runtime.h>
+
+#include "device_util.cuh"
+#include "ksvd_internal.cuh"
+
+namespace ksvd {
+
+constexpr int kTP = 32;         // patches per tile
+constexpr int kOmpThreads = 256;
+constexpr int kAtomBlock = 256;  // atoms per register-tiled pass (32 groups x 8)
+constexpr int kLMax = 32;        // omp_iter limit (support list fits a warp)
+
+struct OmpLayout {
+  int Kpad, dks, rks;
+  size_t off_dk, off_rk, off_ys, off_lc, off_bv, off_s, off_gam, off_sel, off_cnt, off_done, off_redv, off_redi,
+      total;
+};
+
+__host__ __device__ inline size_t al16(size_t x) { return (x + 15) & ~size_t(15); }
+
+__host__ __device__ inline OmpLayout omp_layout(int n, int K, int L) {
+  OmpLayout o;
+  o.Kpad = (K + kAtomBlock - 1) / kAtomBlock * kAtomBlock;
+  o.dks = o.Kpad + 4;
+  o.rks = kTP + 4;
+  size_t off = 0;
+  o.off_dk = off;
+  off = al16(off + size_t(n) * o.dks * 4);
+  o.off_rk = off;
+  off = al16(off + size_t(n) * o.rks * 4);
+  o.off_ys = off;
+  off = al16(off + size_t(kTP) * n * 4);
+  o.off_lc = off;
+  off = al16(off + size_t(kTP) * L * L * 8);
+  o.off_bv = off;
+  off = al16(off + size_t(kTP) * L * 8);
+  o.off_s = off;
+  off = al16(off + size_t(kTP) * L * 4);
+  o.off_gam = off;
+  off = al16(off + size_t(kTP) * L * 4);
+  o.off_sel = off;
+  off = al16(off + kTP * 4);
+  o.off_cnt = off;
+  off = al16(off + kTP * 4);
+  o.off_done = off;
+  off = al16(off + kTP * 4);
+  o.off_redv = off;
+  off = al16(off + 8 * kTP * 4);
+  o.off_redi = off;
+  off = al16(off + 8 * kTP * 4);
+  o.total = off;
+  return o;
+}
+
+__device__ __forceinline__ bool better(float v1, int i1, float v2, int i2) {
+  return v1 > v2 || (v1 == v2 && i1 < i2);
+}
+
+__global__ void __launch_bounds__(kOmpThreads, 1)
+    omp_fp32_kernel(const float* __restrict__ Y, int64_t N, int n, const float* __restrict__ D,
+                    const double* __restrict__ Gram, int K, int L, int32_t* __restrict__ idx_out,
+                    float* __restrict__ coef_out, int64_t ntiles) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const OmpLayout lo = omp_layout(n, K, L);
+  float* Dk = reinterpret_cast<float*>(smem + lo.off_dk);
+  float* Rk = reinterpret_cast<float*>(smem + lo.off_rk);
+  float* Ys = reinterpret_cast<float*>(smem + lo.off_ys);
+  double* Lc = reinterpret_cast<double*>(smem + lo.off_lc);
+  double* bvec = reinterpret_cast<double*>(smem + lo.off_bv);
+  int* S = reinterpret_cast<int*>(smem + lo.off_s);
+  float* gam = reinterpret_cast<float*>(smem + lo.off_gam);
+  int* sel = reinterpret_cast<int*>(smem + lo.off_sel);
+  int* cnt = reinterpret_cast<int*>(smem + lo.off_cnt);
+  int* done = reinterpret_cast<int*>(smem + lo.off_done);
+  float* redv = reinterpret_cast<float*>(smem + lo.off_redv);
+  int* redi = reinterpret_cast<int*>(smem + lo.off_redi);
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int dks = lo.dks, rks = lo.rks, Kpad = lo.Kpad;
+
+  // Dictionary, k-major, padded atoms zero.
+  for (int t = tid; t < K * n; t += kOmpThreads) {
+    int a = t / n, k = t - a * n;
+    Dk[k * dks + a] = __ldg(D + t);
+  }
+  if (Kpad > K) {
+    const int padw = Kpad - K;
+    for (int t = tid; t < n * padw; t += kOmpThreads) {
+      int k = t / padw, a = K + (t - k * padw);
+      Dk[k * dks + a] = 0.0f;
+    }
+  }
+  __syncthreads();
+
+  const int ag = tid >> 3, pg = tid & 7;  // atom group (32), patch group (8)
+
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t p0 = tile * kTP;
+    const int np = (N - p0 < kTP) ? int(N - p0) : kTP;
+    const float* Yt = Y + p0 * n;
+    for (int t = tid; t < kTP * n; t += kOmpThreads) {
+      int p = t / n, k = t - p * n;
+      float v = (p < np) ? __ldg(Yt + t) : 0.0f;
+      Ys[t] = v;
+      Rk[k * rks + p] = v;
+    }
+    if (tid < kTP) {
+      cnt[tid] = 0;
+      done[tid] = (tid >= np);
+    }
+    __syncthreads();
+
+    for (int step = 0; step < L; ++step) {
+      const int active = (tid < kTP) ? !done[tid] : 0;
+      if (!__syncthreads_or(active)) break;
+
+      // ---- correlation D^T R and per-thread argmax ------------------------
+      float bv[4];
+      int bi[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        bv[j] = -1.0f;
+        bi[j] = 0x7fffffff;
+      }
+      for (int ab = 0; ab < Kpad; ab += kAtomBlock) {
+        float acc[8][4];
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
+        const float* dcol = Dk + ab + ag * 8;
+        const float* rcol = Rk + pg * 4;
+#pragma unroll 4
+        for (int k = 0; k < n; ++k) {
+          const float4 d0 = *reinterpret_cast<const float4*>(dcol + k * dks);
+          const float4 d1 = *reinterpret_cast<const float4*>(dcol + k * dks + 4);
+          const float4 r = *reinterpret_cast<const float4*>(rcol + k * rks);
+          const float dv[8] = {d0.x, d0.y, d0.z, d0.w, d1.x, d1.y, d1.z, d1.w};
+          const float rv[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+          for (int i = 0; i < 8; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(dv[i], rv[j], acc[i][j]);
+        }
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const int a = ab + ag * 8 + i;
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const float v = fabsf(acc[i][j]);
+            if (a < K && v > bv[j]) {
+              bv[j] = v;
+              bi[j] = a;
+            }
+          }
+        }
+      }
+      // reduce over the 4 atom groups of the warp (lanes 8 and 16 apart)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+#pragma unroll
+        for (int off = 8; off <= 16; off <<= 1) {
+          float ov = __shfl_xor_sync(0xffffffffu, bv[j], off);
+          int oi = __shfl_xor_sync(0xffffffffu, bi[j], off);
+          if (better(ov, oi, bv[j], bi[j])) {
+            bv[j] = ov;
+            bi[j] = oi;
+          }
+        }
+      }
+      if (lane < 8) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          redv[warp * kTP + pg * 4 + j] = bv[j];
+          redi[warp * kTP + pg * 4 + j] = bi[j];
+        }
+      }
+      __syncthreads();
+      if (tid < kTP) {
+        float v = redv[tid];
+        int i = redi[tid];
+        for (int w = 1; w < 8; ++w) {
+          float ov = redv[w * kTP + tid];
+          int oi = redi[w * kTP + tid];
+          if (better(ov, oi, v, i)) {
+            v = ov;
+            i = oi;
+          }
+        }
+        sel[tid] = (i < K) ? i : 0;
+      }
+      __syncthreads();
+
+      // ---- least squares on the grown support, residual, norm -------------
+      for (int q = 0; q < kTP / 8; ++q) {
+        const int p = warp + 8 * q;
+        if (done[p]) continue;
+        const int a = sel[p];
+        const int k = cnt[p];
+        const bool dup = (lane < k) && (S[p * L + lane] == a);
+        if (__any_sync(0xffffffffu, dup)) {
+          if (lane == 0) done[p] = 1;
+          continue;
+        }
+        // b = d_a . y in FP64
+        double bp = 0.0;
+        const float* da = D + int64_t(a) * n;
+        const float* yp = Ys + p * n;
+        for (int i = lane; i < n; i += 32) bp = fma(double(__ldg(da + i)), double(yp[i]), bp);
+        bp = warp_sum(bp);
+        int ok = 1;
+        if (lane == 0) {
+          double* Lp = Lc + p * L * L;
+          double ww = 0.0;
+          for (int i = 0; i < k; ++i) {
+            double s = Gram[int64_t(S[p * L + i]) * K + a];
+            for (int j = 0; j < i; ++j) s -= Lp[i * L + j] * Lp[k * L + j];
+            double wi = s / Lp[i * L + i];
+            Lp[k * L + i] = wi;
+            ww += wi * wi;
+          }
+          double piv2 = Gram[int64_t(a) * K + a] - ww;
+          if (!(piv2 > 0.0)) {
+            ok = 0;
+          } else {
+            Lp[k * L + k] = sqrt(piv2);
+            S[p * L + k] = a;
+            bvec[p * L + k] = bp;
+            cnt[p] = k + 1;
+            // solve L L^T g = b
+            double yv[kLMax];
+            for (int i = 0; i <= k; ++i) {
+              double s = bvec[p * L + i];
+              for (int j = 0; j < i; ++j) s -= Lp[i * L + j] * yv[j];
+              yv[i] = s / Lp[i * L + i];
+            }
+            for (int i = k; i >= 0; --i) {
+              double s = yv[i];
+              for (int j = i + 1; j <= k; ++j) s -= Lp[j * L + i] * yv[j];
+              yv[i] = s / Lp[i * L + i];
+            }
+            for (int i = 0; i <= k; ++i) gam[p * L + i] = float(yv[i]);
+          }
+        }
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (!ok) {
+          if (lane == 0) done[p] = 1;
+          continue;
+        }
+        __syncwarp();
+        const int kk = k + 1;
+        float nrm = 0.0f;
+        for (int i = lane; i < n; i += 32) {
+          float r = yp[i];
+          for (int s = 0; s < kk; ++s) r = fmaf(-gam[p * L + s], __ldg(D + int64_t(S[p * L + s]) * n + i), r);
+          Rk[i * rks + p] = r;
+          nrm = fmaf(r, r, nrm);
+        }
+        nrm = warp_sum(nrm);
+        if (lane == 0 && sqrtf(nrm) < 1e-3f) done[p] = 1;
+      }
+      __syncthreads();
+    }
+
+    // ---- compact codes ------------------------------------------------------
+    for (int t = tid; t < np * L; t += kOmpThreads) {
+      const int p = t / L, s = t - p * L;
+      const bool used = s < cnt[p];
+      idx_out[(p0 + p) * L + s] = used ? S[p * L + s] : -1;
+      coef_out[(p0 + p) * L + s] = used ? gam[p * L + s] : 0.0f;
+    }
+    __syncthreads();
+  }
+}
+
+size_t omp_fp32_smem_bytes(int n, int K, int L) { return omp_layout(n, K, L).total; }
+
+bool omp_fp32_supported(int n, int K, int L) {
+  return L >= 1 && L <= kLMax && n >= 1 && K >= 1 && omp_fp32_smem_bytes(n, K, L) <= 227 * 1024;
+}
+
+cudaError_t launch_omp_fp32(const float* patches, int64_t N, int n, const float* dict, const double* gram, int K,
+                            int L, int32_t* idx, float* coef, int num_sms, cudaStream_t s) {
+  size_t smem = omp_fp32_smem_bytes(n, K, L);
+  cudaError_t e = cudaFuncSetAttribute(omp_fp32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  int64_t ntiles = (N + kTP - 1) / kTP;
+  int grid = int(std::min<int64_t>(ntiles, num_sms));
+  omp_fp32_kernel<<<grid, kOmpThreads, smem, s>>>(patches, N, n, dict, gram, K, L, idx, coef, ntiles);
+  return cudaGetLastError();
+}
+
+}  // namespace ksvd

@@ -1,0 +1,128 @@
+// Internal declarations shared by the CUDA translation units of ksvd_sm100.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "ksvd_sm100.h"
+
+namespace ksvd {
+
+// ---------------------------------------------------------------------------
+// Device-side error codes written to the context's flag word.
+// ---------------------------------------------------------------------------
+enum DevErr : int {
+  DEVERR_NONE = 0,
+  DEVERR_TIMEOUT = 1,    // a bounded grid-barrier wait gave up
+  DEVERR_ZERO_ATOM = 2,  // an initial atom had zero norm
+  DEVERR_BAD_INDEX = 3,  // a code index outside [0, K)
+};
+
+// State of the software grid barrier used by the persistent cooperative
+// kernels.  Reset by the host before every launch.
+struct GridBarrier {
+  unsigned int count;
+  unsigned int gen;
+  int err;
+  int pad;
+};
+
+// Counters the kernels report back (device memory, reset per call).
+struct DevStats {
+  unsigned long long power_iters;
+  unsigned long long atoms_updated;
+  unsigned long long omp_rescore_misses;
+  unsigned long long pad;
+};
+
+// ---------------------------------------------------------------------------
+// Kernel launchers (each returns the launch's cudaError_t).
+// ---------------------------------------------------------------------------
+struct PatchGeom {
+  int W, H;     // image width (x) and height (y)
+  int pw, ph;   // patchWidthDim (extent along y), patchHeightDim (along x)
+  int sw, sh;   // slidingWidth (step along y), slidingHeight (step along x)
+  int nx, ny;   // patch positions along x (outer) and y (inner)
+  int64_t N;    // nx * ny
+  int n;        // pw * ph
+};
+
+bool make_geom(int W, int H, int pw, int ph, int sw, int sh, PatchGeom* g);
+
+cudaError_t launch_im2col(const float* img, const PatchGeom& g, float* patches, cudaStream_t s);
+cudaError_t launch_log2_image(const float* in, float* out, int64_t count, cudaStream_t s);
+cudaError_t launch_init_dict(const float* patches, int64_t N, int n, int K, int int_norm, float* dict,
+                             GridBarrier* flags, cudaStream_t s);
+cudaError_t launch_gram_f64(const float* dict, int K, int n, double* gram, cudaStream_t s);
+cudaError_t launch_codes_to_dense(const int32_t* idx, const float* coef, int64_t N, int L, int K,
+                                  float* dense, cudaStream_t s);
+
+// OMP (FP32 SIMT correlation).  gram: K x K doubles from launch_gram_f64.
+size_t omp_fp32_smem_bytes(int n, int K, int L);
+bool omp_fp32_supported(int n, int K, int L);
+cudaError_t launch_omp_fp32(const float* patches, int64_t N, int n, const float* dict, const double* gram,
+                            int K, int L, int32_t* idx, float* coef, int num_sms, cudaStream_t s);
+
+// Dictionary update.
+struct CsrWork {
+  int* chunk_counts;   // nchunks x K
+  int* atom_ptr;       // K + 1
+  int* entries;        // N * L (patch * L + slot), grouped by atom, ascending patch
+  int64_t nchunks;
+};
+int64_t csr_num_chunks(int64_t N);
+cudaError_t launch_csr_build(const int32_t* idx, const float* coef, int64_t N, int L, int K, CsrWork w,
+                             cudaStream_t s);
+bool update_supported(int n);
+size_t update_smem_bytes(int n);
+int update_grid_size(int n, int num_sms);
+cudaError_t launch_update(const float* patches, int64_t N, int n, float* dict, int K, int L,
+                          const int32_t* idx, float* coef, CsrWork w, int q1_cap, float* gpart,
+                          float* gsum, GridBarrier* bar, DevStats* stats, int grid, cudaStream_t s);
+
+// Image rebuild.
+cudaError_t launch_col2im(const float* noisy, const PatchGeom& g, const float* dict, int K, int L,
+                          const int32_t* idx, const float* coef, float* acc, double* partials,
+                          int* num_partials, cudaStream_t s);
+int col2im_num_tiles(const PatchGeom& g);
+cudaError_t launch_blend(const float* noisy, const PatchGeom& g, const float* acc, const double* partials,
+                         int num_partials, double sigma2, int speckle, float* out, double* lambda_dev,
+                         cudaStream_t s);
+
+}  // namespace ksvd
+
+// ---------------------------------------------------------------------------
+// The context behind the opaque ksvd_ctx handle.
+// ---------------------------------------------------------------------------
+struct ksvd_ctx {
+  ksvd_params p{};
+  int device = 0;
+  int num_sms = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  std::string err;
+
+  // Named device buffers, grown on demand and kept until ksvd_destroy.
+  struct Buf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+  };
+  std::map<std::string, Buf> bufs;
+
+  // Per-kernel-family device timing.
+  struct Family {
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
+    double total_ms = 0.0;
+    int64_t launches = 0;
+  };
+  bool profiling = false;
+  std::map<std::string, Family> families;
+  std::vector<cudaEvent_t> event_pool;
+  int64_t launch_count = 0;
+
+  ksvd::GridBarrier* d_flags = nullptr;  // error flag word + barrier
+  ksvd::DevStats* d_stats = nullptr;
+};

@@ -1,0 +1,299 @@
+"""ctypes bindings to the ksvd_sm100 C ABI (include/ksvd_sm100.h).
+
+Device buffers are torch CUDA tensors (torch provides device memory and
+streams only); every computation runs in libksvd_sm100.so.  There is no CPU
+fallback: if the library or a GPU is missing the calls raise.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+PKG_DIR = Path(__file__).resolve().parent
+LIB_PATH = PKG_DIR / "libksvd_sm100.so"
+HEADER = PKG_DIR.parent / "include" / "ksvd_sm100.h"
+
+# ksvd_type
+CUDA_K_GESVD, CUDA_K_GESVDJ, CUDA_K_GESVDA, CUDA_K_SM100A = 0, 1, 2, 3
+# ksvd_status
+OK, ERR_LOAD, ERR_DENOISE, ERR_SAVE = 0, -1, -2, -3
+ERR_INVALID, ERR_CUDA, ERR_NO_MEMORY, ERR_TIMEOUT, ERR_NUMERIC, ERR_NO_DEVICE = -10, -11, -12, -13, -14, -15
+# ksvd_precision
+PREC_FP32, PREC_BF16_RESCORE = 0, 1
+# compat flags
+COMPAT_INT_NORM, COMPAT_Q1_CAP = 0x1, 0x2
+COMPAT_REFERENCE = COMPAT_INT_NORM | COMPAT_Q1_CAP
+
+
+class KsvdParams(ctypes.Structure):
+    _fields_ = [
+        ("patch_width_dim", ctypes.c_int),
+        ("patch_height_dim", ctypes.c_int),
+        ("sliding_width", ctypes.c_int),
+        ("sliding_height", ctypes.c_int),
+        ("atoms", ctypes.c_int),
+        ("ksvd_iter", ctypes.c_int),
+        ("omp_iter", ctypes.c_int),
+        ("bw", ctypes.c_int),
+        ("speckle", ctypes.c_int),
+        ("type", ctypes.c_int),
+        ("min_omp_iter_batch", ctypes.c_int),
+        ("sub_image_width_dim", ctypes.c_int),
+        ("sub_image_height_dim", ctypes.c_int),
+        ("precision", ctypes.c_int),
+        ("compat", ctypes.c_uint),
+        ("device", ctypes.c_int),
+    ]
+
+
+class KsvdStats(ctypes.Structure):
+    _fields_ = [
+        ("init_ms", ctypes.c_int64),
+        ("working_ms", ctypes.c_int64),
+        ("finalize_ms", ctypes.c_int64),
+        ("num_patches", ctypes.c_int64),
+        ("lambda_", ctypes.c_double),
+        ("iter_ms", ctypes.c_double),
+        ("final_omp_ms", ctypes.c_double),
+        ("extract_ms", ctypes.c_double),
+        ("build_ms", ctypes.c_double),
+        ("power_iters", ctypes.c_int64),
+        ("atoms_updated", ctypes.c_int64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class KsvdError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"ksvd status {status}: {message}")
+        self.status = status
+
+
+_lib = None
+_vp = ctypes.c_void_p
+_i64 = ctypes.c_int64
+_int = ctypes.c_int
+
+
+def build() -> Path:
+    """Compile libksvd_sm100.so in-tree (make -C <package>)."""
+    subprocess.run(["make", "-s", "-j8", "-C", str(PKG_DIR)], check=True)
+    return LIB_PATH
+
+
+def lib():
+    """Load the library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise FileNotFoundError(f"{LIB_PATH} is missing: build it with make -C {PKG_DIR}")
+        L = ctypes.CDLL(str(LIB_PATH))
+        P = ctypes.POINTER(KsvdParams)
+        L.ksvd_abi_version.restype = _int
+        L.ksvd_params_default.argtypes = [P]
+        L.ksvd_type_from_string.argtypes = [ctypes.c_char_p, ctypes.POINTER(_int)]
+        L.ksvd_type_from_string.restype = _int
+        L.ksvd_type_name.argtypes = [_int]
+        L.ksvd_type_name.restype = ctypes.c_char_p
+        L.ksvd_status_string.argtypes = [_int]
+        L.ksvd_status_string.restype = ctypes.c_char_p
+        L.ksvd_num_patches.argtypes = [P, _int, _int]
+        L.ksvd_num_patches.restype = _i64
+        L.ksvd_create.argtypes = [P, ctypes.POINTER(_vp)]
+        L.ksvd_create.restype = _int
+        L.ksvd_destroy.argtypes = [_vp]
+        L.ksvd_last_error.argtypes = [_vp]
+        L.ksvd_last_error.restype = ctypes.c_char_p
+        L.ksvd_set_stream.argtypes = [_vp, _vp]
+        L.ksvd_set_stream.restype = _int
+        L.ksvd_get_stream.argtypes = [_vp]
+        L.ksvd_get_stream.restype = _vp
+        L.ksvd_denoise.argtypes = [_vp, _vp, _int, _int, ctypes.c_float, _vp, ctypes.POINTER(KsvdStats)]
+        L.ksvd_denoise.restype = _int
+        L.ksvd_extract_patches.argtypes = [_vp, _vp, _int, _int, _vp]
+        L.ksvd_extract_patches.restype = _int
+        L.ksvd_init_dictionary.argtypes = [_vp, _vp, _i64, _vp]
+        L.ksvd_init_dictionary.restype = _int
+        L.ksvd_omp.argtypes = [_vp, _vp, _i64, _vp, _vp, _vp]
+        L.ksvd_omp.restype = _int
+        L.ksvd_update_dictionary.argtypes = [_vp, _vp, _i64, _vp, _vp, _vp]
+        L.ksvd_update_dictionary.restype = _int
+        L.ksvd_iterate.argtypes = [_vp, _vp, _i64, _vp, _vp, _vp, _int]
+        L.ksvd_iterate.restype = _int
+        L.ksvd_build_image.argtypes = [_vp, _vp, _int, _int, ctypes.c_float, _vp, _vp, _vp, _i64, _vp,
+                                       ctypes.POINTER(ctypes.c_double)]
+        L.ksvd_build_image.restype = _int
+        L.ksvd_codes_to_dense.argtypes = [_vp, _vp, _vp, _i64, _vp]
+        L.ksvd_codes_to_dense.restype = _int
+        L.ksvd_profile_enable.argtypes = [_vp, _int]
+        L.ksvd_profile_enable.restype = _int
+        L.ksvd_profile_read.argtypes = [_vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_double),
+                                        ctypes.POINTER(_i64)]
+        L.ksvd_profile_read.restype = _int
+        L.ksvd_profile_reset.argtypes = [_vp]
+        L.ksvd_profile_reset.restype = _int
+        L.ksvd_launch_count.argtypes = [_vp]
+        L.ksvd_launch_count.restype = _i64
+        _lib = L
+    return _lib
+
+
+def default_params() -> KsvdParams:
+    p = KsvdParams()
+    lib().ksvd_params_default(ctypes.byref(p))
+    return p
+
+
+def make_params(**kw) -> KsvdParams:
+    p = default_params()
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, int(v))
+    return p
+
+
+def type_from_string(name: str):
+    known = _int(0)
+    t = lib().ksvd_type_from_string(name.encode(), ctypes.byref(known))
+    return t, bool(known.value)
+
+
+def num_patches(params: KsvdParams, width: int, height: int) -> int:
+    return int(lib().ksvd_num_patches(ctypes.byref(params), width, height))
+
+
+def _ptr(t) -> int:
+    """Device pointer of a torch tensor (checked to be CUDA + contiguous)."""
+    if not t.is_cuda:
+        raise ValueError("expected a CUDA tensor")
+    if not t.is_contiguous():
+        raise ValueError("expected a contiguous tensor")
+    return t.data_ptr()
+
+
+class Context:
+    """Owns one ksvd_ctx.  Stage methods take torch CUDA tensors."""
+
+    def __init__(self, params: KsvdParams | None = None, **kw):
+        self.params = params if params is not None else make_params(**kw)
+        h = _vp()
+        st = lib().ksvd_create(ctypes.byref(self.params), ctypes.byref(h))
+        if st != OK:
+            raise KsvdError(st, lib().ksvd_status_string(st).decode())
+        self.h = h
+
+    # -- lifetime ---------------------------------------------------------
+    def close(self):
+        if getattr(self, "h", None):
+            lib().ksvd_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int):
+        if st != OK:
+            raise KsvdError(st, lib().ksvd_last_error(self.h).decode())
+
+    # -- properties -------------------------------------------------------
+    @property
+    def n(self) -> int:
+        return self.params.patch_width_dim * self.params.patch_height_dim
+
+    @property
+    def K(self) -> int:
+        return self.params.atoms
+
+    @property
+    def L(self) -> int:
+        return self.params.omp_iter
+
+    def set_stream(self, stream_handle: int | None):
+        self._check(lib().ksvd_set_stream(self.h, stream_handle))
+
+    # -- stages (device tensors) ------------------------------------------
+    def extract_patches(self, img, out):
+        H, W = img.shape
+        self._check(lib().ksvd_extract_patches(self.h, _ptr(img), W, H, _ptr(out)))
+
+    def init_dictionary(self, patches, dict_out):
+        self._check(lib().ksvd_init_dictionary(self.h, _ptr(patches), patches.shape[0], _ptr(dict_out)))
+
+    def omp(self, patches, dictionary, idx, coef):
+        self._check(lib().ksvd_omp(self.h, _ptr(patches), patches.shape[0], _ptr(dictionary), _ptr(idx),
+                                   _ptr(coef)))
+
+    def update_dictionary(self, patches, dictionary, idx, coef):
+        self._check(lib().ksvd_update_dictionary(self.h, _ptr(patches), patches.shape[0], _ptr(dictionary),
+                                                 _ptr(idx), _ptr(coef)))
+
+    def iterate(self, patches, dictionary, idx, coef, iters: int):
+        self._check(lib().ksvd_iterate(self.h, _ptr(patches), patches.shape[0], _ptr(dictionary), _ptr(idx),
+                                       _ptr(coef), int(iters)))
+
+    def build_image(self, noisy, sigma2, dictionary, idx, coef, out) -> float:
+        H, W = noisy.shape
+        lam = ctypes.c_double(0.0)
+        self._check(lib().ksvd_build_image(self.h, _ptr(noisy), W, H, float(sigma2), _ptr(dictionary), _ptr(idx),
+                                           _ptr(coef), idx.shape[0], _ptr(out), ctypes.byref(lam)))
+        return lam.value
+
+    def codes_to_dense(self, idx, coef, dense):
+        self._check(lib().ksvd_codes_to_dense(self.h, _ptr(idx), _ptr(coef), idx.shape[0], _ptr(dense)))
+
+    # -- whole denoise (host buffers) -------------------------------------
+    def denoise(self, img: np.ndarray, sigma2: float, out: np.ndarray | None = None):
+        img = np.ascontiguousarray(img, dtype=np.float32)
+        H, W = img.shape
+        if out is None:
+            out = np.empty_like(img)
+        st = KsvdStats()
+        self._check(lib().ksvd_denoise(self.h, img.ctypes.data, W, H, float(sigma2), out.ctypes.data,
+                                       ctypes.byref(st)))
+        return out, st.as_dict()
+
+    def denoise_ptr(self, img_ptr: int, W: int, H: int, sigma2: float, out_ptr: int) -> KsvdStats:
+        """Host-pointer form (e.g. pinned torch tensors)."""
+        st = KsvdStats()
+        self._check(lib().ksvd_denoise(self.h, img_ptr, W, H, float(sigma2), out_ptr, ctypes.byref(st)))
+        return st
+
+    # -- profiling --------------------------------------------------------
+    def profile(self, enable: bool = True):
+        self._check(lib().ksvd_profile_enable(self.h, int(enable)))
+
+    def profile_reset(self):
+        self._check(lib().ksvd_profile_reset(self.h))
+
+    def profile_read(self, family: str):
+        ms = ctypes.c_double(0.0)
+        n = _i64(0)
+        self._check(lib().ksvd_profile_read(self.h, family.encode(), ctypes.byref(ms), ctypes.byref(n)))
+        return ms.value, n.value
+
+    def launch_count(self) -> int:
+        return int(lib().ksvd_launch_count(self.h))
+
+
+def declared_symbols() -> list[str]:
+    """Function names declared in include/ksvd_sm100.h."""
+    import re
+    txt = HEADER.read_text()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(ksvd_[a-z0-9_]+)\s*\(", txt)))

@@ -1,0 +1,208 @@
+/*
+ * ksvd_sm100 — C ABI of the B200 (sm_100a) K-SVD denoiser.
+ *
+ * Drop-in boundary for the hot path of newfla/CUDA-K-SVD-Denoising's
+ * denoisingLib: patch extraction, dictionary initialisation, the K-SVD
+ * iteration (OMP sparse coding + sequential per-atom dictionary update) and
+ * the image rebuild.  Every entry point takes plain pointers and sizes.
+ *
+ * Layouts (the reference's column-major matrices, src/lib/baseUtilityLib/
+ * baseUtilityLib.h:16-36, stored as contiguous rows here):
+ *   image    : height x width floats, row-major (pixel (x, y) at y*width + x)
+ *   patches  : N x n floats, one contiguous patch per row (the reference's
+ *              n x N column-major "noisePatches"), n = patchWidthDim *
+ *              patchHeightDim; element r*patchWidthDim + c of patch (ix, iy)
+ *              is pixel (x = ix*slidingHeight + r, y = iy*slidingWidth + c),
+ *              patch index ix*ny + iy (cuda_svd_denoiser.cu:221-256)
+ *   dict     : K x n floats, one unit-norm atom per row (the reference's n x K
+ *              "dictionary")
+ *   codes    : compact sparse code, idx N x L int32 (atom, or -1 for an unused
+ *              slot) and coef N x L floats; the reference keeps the same values
+ *              in a dense K x N matrix (cublas_matrix_omp.cu:79);
+ *              ksvd_codes_to_dense() produces that layout.
+ *
+ * Pointers named d_* are device pointers on the context's device; all work
+ * is ordered on the context's stream (ksvd_set_stream).  Functions without
+ * d_* arguments take host memory.
+ *
+ * Status values 0, -1, -2, -3 keep the meaning of the reference's
+ * CudaKSvdDenoiser::denoising() result (cuda_svd_denoiser.cu:86-102).
+ */
+#ifndef KSVD_SM100_H
+#define KSVD_SM100_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KSVD_ABI_VERSION 1
+
+/* Replaces denoising::DenoiserType (src/lib/denoisingLib/denoisingLib.h:21).
+ * The three cuSOLVER-backed values are accepted and run the sm_100a path
+ * (they only chose the SVD engine used in the dictionary update,
+ * cuda_svd_denoiser.cu:72-84); KSVD_CUDA_K_SM100A names it explicitly. */
+typedef enum ksvd_type {
+  KSVD_CUDA_K_GESVD = 0,
+  KSVD_CUDA_K_GESVDJ = 1,
+  KSVD_CUDA_K_GESVDA = 2,
+  KSVD_CUDA_K_SM100A = 3
+} ksvd_type;
+
+typedef enum ksvd_status {
+  KSVD_OK = 0,
+  KSVD_ERR_LOAD = -1,     /* image could not be loaded        (denoising() -1) */
+  KSVD_ERR_DENOISE = -2,  /* denoising failed                 (denoising() -2) */
+  KSVD_ERR_SAVE = -3,     /* image could not be saved         (denoising() -3) */
+  KSVD_ERR_INVALID = -10, /* bad argument or parameter combination             */
+  KSVD_ERR_CUDA = -11,    /* a CUDA call failed (see ksvd_last_error)          */
+  KSVD_ERR_NO_MEMORY = -12,
+  KSVD_ERR_TIMEOUT = -13, /* a bounded device wait gave up                     */
+  KSVD_ERR_NUMERIC = -14, /* zero-norm initial atom or non-finite data         */
+  KSVD_ERR_NO_DEVICE = -15
+} ksvd_status;
+
+/* Arithmetic of the OMP correlation D^T R. */
+typedef enum ksvd_precision {
+  KSVD_PREC_FP32 = 0,        /* plain FP32 FMA                                 */
+  KSVD_PREC_BF16_RESCORE = 1 /* BF16 tensor cores, FP32 re-score of top hits */
+} ksvd_precision;
+
+/* Reference behaviours reproduced on request (bit flags for ksvd_params.compat). */
+#define KSVD_COMPAT_INT_NORM 0x1u /* initDictionary sums squares into an int
+                                     accumulator (cuda_svd_denoiser.cu:59)   */
+#define KSVD_COMPAT_Q1_CAP 0x2u   /* only the first 1024 patches of an atom's
+                                     support enter its update
+                                     (cuda_svd_denoiser.cu:295-296,315,324)   */
+#define KSVD_COMPAT_REFERENCE (KSVD_COMPAT_INT_NORM | KSVD_COMPAT_Q1_CAP)
+
+/* Mirrors denoising::Denoiser's parameters (denoisingLib.h:44-56) and the
+ * config.json globalParams keys (batch_denoiser.cpp:60-73). */
+typedef struct ksvd_params {
+  int patch_width_dim;      /* "patchWidthDim"     default 8  */
+  int patch_height_dim;     /* "patchHeightDim"    default 8  */
+  int sliding_width;        /* "slidingWidth"      default 2  */
+  int sliding_height;       /* "slidingHeight"     default 2  */
+  int atoms;                /* "atoms"             default 256 */
+  int ksvd_iter;            /* "ksvdIter"          default 10 */
+  int omp_iter;             /* "ompIter"           default 5  */
+  int bw;                   /* "B&W"               default 1  */
+  int speckle;              /* "speckle"           default 0  */
+  int type;                 /* "type" (ksvd_type)  default KSVD_CUDA_K_SM100A */
+  int min_omp_iter_batch;   /* "minOmpIterBatch"   accepted, no effect here */
+  int sub_image_width_dim;  /* "subImageWidthDim"  default 0  */
+  int sub_image_height_dim; /* "subImageHeightDim" default 0  */
+  int precision;            /* ksvd_precision      default KSVD_PREC_FP32 */
+  unsigned compat;          /* KSVD_COMPAT_*       default KSVD_COMPAT_REFERENCE */
+  int device;               /* CUDA device ordinal default 0 */
+} ksvd_params;
+
+/* Timings in ms (TimeElapsed, baseUtilityLib.h:38-44) and a few counters. */
+typedef struct ksvd_stats {
+  int64_t init_ms;
+  int64_t working_ms;
+  int64_t finalize_ms;
+  int64_t num_patches;
+  double lambda;         /* blend weight of createImage */
+  double iter_ms;        /* device time of the K-SVD iterations (OMP + update) */
+  double final_omp_ms;   /* device time of the final OMP */
+  double extract_ms;     /* device time of the patch gather */
+  double build_ms;       /* device time of the image rebuild */
+  int64_t power_iters;   /* power iterations spent in the last update sweep */
+  int64_t atoms_updated; /* atoms with a non-empty support in the last sweep */
+} ksvd_stats;
+
+typedef struct ksvd_ctx ksvd_ctx;
+
+/* Defaults of denoisingLib.h:44-56 (type/precision/compat as documented). */
+void ksvd_params_default(ksvd_params* p);
+
+/* "CUDA_K_GESVD" / "CUDA_K_GESVDJ" / "CUDA_K_GESVDA" / "CUDA_K_SM100A" ->
+ * ksvd_type.  Replaces DenoiserTypeMap (denoisingLib.h:23-31); like the
+ * reference's std::map::operator[], an unknown name yields 0 (CUDA_K_GESVD).
+ * *known is set to 1 for a listed name, 0 otherwise (may be NULL). */
+int ksvd_type_from_string(const char* name, int* known);
+const char* ksvd_type_name(int type);
+
+/* Replaces Denoiser::factory (denoiser.cpp:108-127) + the parameter copy of
+ * BatchDenoiser::factory (batch_denoiser.cpp:385-399).  Validates p, selects
+ * the device and creates the context's stream.  Device memory is allocated
+ * on first use and kept for the life of the context. */
+ksvd_status ksvd_create(const ksvd_params* p, ksvd_ctx** out);
+void ksvd_destroy(ksvd_ctx* ctx);
+const char* ksvd_last_error(const ksvd_ctx* ctx);
+const char* ksvd_status_string(int status);
+int ksvd_abi_version(void);
+
+/* Work is ordered on this stream (cudaStream_t passed as void*; NULL means
+ * the context's own stream). */
+ksvd_status ksvd_set_stream(ksvd_ctx* ctx, void* stream);
+void* ksvd_get_stream(const ksvd_ctx* ctx);
+
+/* Number of patches the parameters give for a width x height image. */
+int64_t ksvd_num_patches(const ksvd_params* p, int width, int height);
+
+/* CudaKSvdDenoiser::denoising() minus file I/O (cuda_svd_denoiser.cu:90-102,
+ * 126-216): host image in, host image out.  sigma2 is the noise variance (the
+ * reference's Denoiser::sigma, denoiser.cpp:56).  For speckle the input is the
+ * linear image; the log2/exp2 transform (denoisingLib.h:124-143) is applied
+ * inside.  Sub-image tiling (subImage*Dim != 0) is honoured. */
+ksvd_status ksvd_denoise(ksvd_ctx* ctx, const float* img, int width, int height, float sigma2,
+                         float* out, ksvd_stats* stats);
+
+/* ---- stage entry points (device pointers) -------------------------------- */
+
+/* createPatches (cuda_svd_denoiser.cu:221-256). d_patches: N x n. */
+ksvd_status ksvd_extract_patches(ksvd_ctx* ctx, const float* d_img, int width, int height,
+                                 float* d_patches);
+
+/* initDictionary + normalizeDictKernel (cuda_svd_denoiser.cu:52-63,261-280):
+ * atoms = patches N/2 .. N/2+K-1 divided by their norm. */
+ksvd_status ksvd_init_dictionary(ksvd_ctx* ctx, const float* d_patches, int64_t num_patches,
+                                 float* d_dict);
+
+/* CuBlasMatrixOmp::work (cublas_matrix_omp.cu:107-402): L = omp_iter atoms per
+ * patch, argmax |D^T r| with lowest-index ties, least squares on the support,
+ * stop when ||r|| < 1e-3. */
+ksvd_status ksvd_omp(ksvd_ctx* ctx, const float* d_patches, int64_t num_patches, const float* d_dict,
+                     int32_t* d_idx, float* d_coef);
+
+/* updateDictionary (cuda_svd_denoiser.cu:285-362): one sequential sweep over
+ * the atoms; d_dict and d_coef are updated in place. */
+ksvd_status ksvd_update_dictionary(ksvd_ctx* ctx, const float* d_patches, int64_t num_patches,
+                                   float* d_dict, const int32_t* d_idx, float* d_coef);
+
+/* kSvd's loop (cuda_svd_denoiser.cu:374-397): iters x (OMP + update), without
+ * the final OMP. */
+ksvd_status ksvd_iterate(ksvd_ctx* ctx, const float* d_patches, int64_t num_patches, float* d_dict,
+                         int32_t* d_idx, float* d_coef, int iters);
+
+/* createImage (cuda_svd_denoiser.cu:413-498) on device: d_noisy is the
+ * (log-domain for speckle) noisy image, d_out the blended image (exp2 applied
+ * for speckle).  *lambda_out (host, may be NULL) receives the blend weight. */
+ksvd_status ksvd_build_image(ksvd_ctx* ctx, const float* d_noisy, int width, int height, float sigma2,
+                             const float* d_dict, const int32_t* d_idx, const float* d_coef,
+                             int64_t num_patches, float* d_out, double* lambda_out);
+
+/* Compact codes -> the reference's dense K x N column-major code matrix
+ * (element (k, p) at p*K + k).  d_dense must hold K*N floats. */
+ksvd_status ksvd_codes_to_dense(ksvd_ctx* ctx, const int32_t* d_idx, const float* d_coef,
+                                int64_t num_patches, float* d_dense);
+
+/* Per-kernel device timing: when enabled, every kernel family records CUDA
+ * events around its launches on the context's stream. */
+ksvd_status ksvd_profile_enable(ksvd_ctx* ctx, int enable);
+/* Sum of launch durations (ms) and launch count of a kernel family since the
+ * last reset ("im2col", "init_dict", "gram", "omp", "csr", "update", "col2im",
+ * ...).  Synchronises the stream. */
+ksvd_status ksvd_profile_read(ksvd_ctx* ctx, const char* family, double* total_ms, int64_t* launches);
+ksvd_status ksvd_profile_reset(ksvd_ctx* ctx);
+/* Total number of kernels this context launched since creation. */
+int64_t ksvd_launch_count(const ksvd_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KSVD_SM100_H */

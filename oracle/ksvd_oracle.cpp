@@ -1,0 +1,637 @@
+// K-SVD CPU oracle — TEST INFRASTRUCTURE ONLY.
+//
+// A plain C++ restatement of the reference's K-SVD denoising hot path
+// (newfla/CUDA-K-SVD-Denoising).  It is used by tests/ to check the CUDA
+// path, by bench.py as the timed CPU baseline ("port"), and nowhere else:
+// the product library never links or calls it.
+//
+// Every function names the reference lines it follows.  The scalar type T is
+// double for the FP64 oracle and float for the FP32 restatement; the tiny
+// dense solves (Cholesky of the support Gram, the n x n eigenproblem) are
+// always done in double.
+//
+// Reference behaviour that is reproduced on purpose (switchable where the
+// reference's behaviour is a defect):
+//  * INT_NORM — initDictionary normalises atoms with a thrust transform_reduce
+//    whose init value is the int literal 0 (cuda_svd_denoiser.cu:59), so the
+//    running sum of squares is converted to int after every addition.
+//  * Q1 cap   — updateDictionary launches copyTransformSparseCodeKernel and
+//    computeErrorKernel with a single 1024-thread block for K <= 1024
+//    (cuda_svd_denoiser.cu:295-296,315,324), so only the first 1024 patches
+//    of an atom's support enter E; the remaining columns of E stay zero
+//    (selectSparseCode is zero-initialised once per sweep at :306 and its
+//    columns >= 1024 are never written), which also sets those patches'
+//    coefficients to zero after the SVD.
+//
+// Deliberate, documented deviations at points where the reference's output
+// is undefined:
+//  * a re-selected atom (argmax lands on an atom already in the support)
+//    ends the pursuit for that patch; the reference would feed a rank-
+//    deficient matrix to gesvda and scatter an arbitrary coefficient
+//    (cublas_matrix_omp.cu:270-347);
+//  * uncovered border pixels (weight 0) are left out of the lambda sum and
+//    returned as the noisy input; the reference divides 0/0 there
+//    (cuda_svd_denoiser.cu:459-463) which makes lambda NaN.
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Host threading: a plain std::thread parallel-for (no OpenMP runtime).
+// par_dynamic hands out chunks from an atomic counter; par_static splits the
+// range into one contiguous block per thread so per-thread partial sums are
+// combined in a fixed order.
+// ---------------------------------------------------------------------------
+int g_threads = 0;
+
+int num_threads() {
+  if (g_threads > 0) return g_threads;
+  unsigned hc = std::thread::hardware_concurrency();
+  return hc ? int(hc) : 1;
+}
+
+template <class F>
+void par_dynamic(int64_t n, int64_t chunk, F&& f) {
+  if (n <= 0) return;
+  int T = int(std::min<int64_t>(num_threads(), (n + chunk - 1) / chunk));
+  std::atomic<int64_t> next(0);
+  auto work = [&]() {
+    for (;;) {
+      int64_t b = next.fetch_add(chunk);
+      if (b >= n) break;
+      f(b, std::min(n, b + chunk));
+    }
+  };
+  if (T <= 1) {
+    work();
+    return;
+  }
+  std::vector<std::thread> th;
+  for (int t = 1; t < T; ++t) th.emplace_back(work);
+  work();
+  for (auto& t : th) t.join();
+}
+
+template <class F>
+void par_static(int64_t n, int T, F&& f) {
+  if (T <= 1 || n <= 1) {
+    f(0, int64_t(0), n);
+    return;
+  }
+  std::vector<std::thread> th;
+  for (int t = 1; t < T; ++t) th.emplace_back([&, t]() { f(t, n * t / T, n * (t + 1) / T); });
+  f(0, int64_t(0), n / T);
+  for (auto& t : th) t.join();
+}
+
+// ---------------------------------------------------------------------------
+// Geometry (cuda_svd_denoiser.cu:221-256).  The reference transposes the
+// image on load (denoiser.cpp:46-51) and walks it with outer index i over x
+// (step slidingHeight, extent patchHeightDim) and inner index j over y (step
+// slidingWidth, extent patchWidthDim).  Patch element e = r*pw + c holds
+// pixel (x = i + r, y = j + c).  For the square images and square patches the
+// reference supports this is exactly its order; the x range is bounded by the
+// image width here (the reference bounds it by the height, identical when
+// square).
+// ---------------------------------------------------------------------------
+struct Geom {
+  int W, H, pw, ph, sw, sh;
+  int nx, ny;  // patch positions along x (outer) and y (inner)
+  int64_t N;
+  int n;
+};
+
+bool make_geom(int W, int H, int pw, int ph, int sw, int sh, Geom* g) {
+  if (W <= 0 || H <= 0 || pw <= 0 || ph <= 0 || sw <= 0 || sh <= 0) return false;
+  if (ph > W || pw > H) return false;
+  g->W = W; g->H = H; g->pw = pw; g->ph = ph; g->sw = sw; g->sh = sh;
+  g->nx = (W - ph) / sh + 1;
+  g->ny = (H - pw) / sw + 1;
+  g->N = int64_t(g->nx) * g->ny;
+  g->n = pw * ph;
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// Small dense linear algebra in double.
+// ---------------------------------------------------------------------------
+
+// Top eigenpair of a symmetric n x n matrix A (row-major, destroyed):
+// Householder reduction to tridiagonal form with accumulated Q, then the
+// implicit QL iteration with shifts on the tridiagonal, rotating Q along.
+// Returns the largest eigenvalue, writes its unit eigenvector to u.
+double sym_top_eig(std::vector<double>& A, int n, double* u) {
+  std::vector<double> Q(size_t(n) * n, 0.0);
+  for (int i = 0; i < n; ++i) Q[size_t(i) * n + i] = 1.0;
+  std::vector<double> v(n), p(n), w(n);
+  for (int k = 0; k + 2 < n; ++k) {
+    // x = A[k+1:, k]
+    double xnorm2 = 0.0;
+    for (int i = k + 1; i < n; ++i) xnorm2 += A[size_t(i) * n + k] * A[size_t(i) * n + k];
+    double xnorm = std::sqrt(xnorm2);
+    if (xnorm == 0.0) continue;
+    double x0 = A[size_t(k + 1) * n + k];
+    double alpha = (x0 >= 0.0) ? -xnorm : xnorm;
+    for (int i = 0; i < n; ++i) v[i] = 0.0;
+    for (int i = k + 1; i < n; ++i) v[i] = A[size_t(i) * n + k];
+    v[k + 1] -= alpha;
+    double vnorm2 = 0.0;
+    for (int i = k + 1; i < n; ++i) vnorm2 += v[i] * v[i];
+    if (vnorm2 == 0.0) continue;
+    double vinv = 1.0 / std::sqrt(vnorm2);
+    for (int i = k + 1; i < n; ++i) v[i] *= vinv;
+    // p = A v (over the trailing block), K = v^T p, w = p - K v
+    for (int i = k; i < n; ++i) {
+      double s = 0.0;
+      for (int j = k + 1; j < n; ++j) s += A[size_t(i) * n + j] * v[j];
+      p[i] = s;
+    }
+    double K = 0.0;
+    for (int i = k + 1; i < n; ++i) K += v[i] * p[i];
+    for (int i = k + 1; i < n; ++i) w[i] = p[i] - K * v[i];
+    // A22 -= 2 v w^T + 2 w v^T
+    for (int i = k + 1; i < n; ++i)
+      for (int j = k + 1; j < n; ++j)
+        A[size_t(i) * n + j] -= 2.0 * (v[i] * w[j] + w[i] * v[j]);
+    A[size_t(k + 1) * n + k] = alpha;
+    A[size_t(k) * n + k + 1] = alpha;
+    for (int i = k + 2; i < n; ++i) {
+      A[size_t(i) * n + k] = 0.0;
+      A[size_t(k) * n + i] = 0.0;
+    }
+    // Q = Q H, H = I - 2 v v^T
+    for (int r = 0; r < n; ++r) {
+      double s = 0.0;
+      for (int j = k + 1; j < n; ++j) s += Q[size_t(r) * n + j] * v[j];
+      s *= 2.0;
+      for (int j = k + 1; j < n; ++j) Q[size_t(r) * n + j] -= s * v[j];
+    }
+  }
+  // Tridiagonal: d[i] = A[i][i], e[i] = A[i+1][i] (e[n-1] = 0).
+  std::vector<double> d(n), e(n, 0.0);
+  for (int i = 0; i < n; ++i) d[i] = A[size_t(i) * n + i];
+  for (int i = 0; i + 1 < n; ++i) e[i] = A[size_t(i + 1) * n + i];
+  // Implicit QL with shifts; columns of Q are rotated with the tridiagonal.
+  for (int l = 0; l < n; ++l) {
+    int iter = 0;
+    int m;
+    do {
+      for (m = l; m < n - 1; ++m) {
+        double dd = std::fabs(d[m]) + std::fabs(d[m + 1]);
+        if (std::fabs(e[m]) <= 1e-300 + 2.220446049250313e-16 * dd) break;
+      }
+      if (m != l) {
+        if (++iter > 200) break;  // never reached for symmetric input
+        double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+        double r = std::hypot(g, 1.0);
+        g = d[m] - d[l] + e[l] / (g + (g >= 0.0 ? r : -r));
+        double s = 1.0, c = 1.0, pp = 0.0;
+        int i;
+        bool deflated = false;
+        for (i = m - 1; i >= l; --i) {
+          double f = s * e[i];
+          double b = c * e[i];
+          r = std::hypot(f, g);
+          e[i + 1] = r;
+          if (r == 0.0) {
+            d[i + 1] -= pp;
+            e[m] = 0.0;
+            deflated = true;
+            break;
+          }
+          s = f / r;
+          c = g / r;
+          g = d[i + 1] - pp;
+          r = (d[i] - g) * s + 2.0 * c * b;
+          pp = s * r;
+          d[i + 1] = g + pp;
+          g = c * r - b;
+          for (int k = 0; k < n; ++k) {
+            double qf = Q[size_t(k) * n + i + 1];
+            double qi = Q[size_t(k) * n + i];
+            Q[size_t(k) * n + i + 1] = s * qi + c * qf;
+            Q[size_t(k) * n + i] = c * qi - s * qf;
+          }
+        }
+        if (deflated) continue;
+        d[l] -= pp;
+        e[l] = g;
+        e[m] = 0.0;
+      }
+    } while (m != l);
+  }
+  int best = 0;
+  for (int i = 1; i < n; ++i)
+    if (d[i] > d[best]) best = i;
+  double nrm = 0.0;
+  for (int k = 0; k < n; ++k) nrm += Q[size_t(k) * n + best] * Q[size_t(k) * n + best];
+  nrm = std::sqrt(nrm);
+  for (int k = 0; k < n; ++k) u[k] = Q[size_t(k) * n + best] / nrm;
+  return d[best];
+}
+
+// Cholesky factor of the support Gram, grown one column at a time.
+// Lc is row-major L x L lower triangular.  Returns false if the new pivot is
+// not positive (the new atom is linearly dependent on the support).
+bool chol_append(double* Lc, int Lmax, int k, const double* g_new, double g_kk) {
+  // Solve Lc[0:k,0:k] w = g_new, then pivot = sqrt(g_kk - w.w)
+  double ww = 0.0;
+  for (int i = 0; i < k; ++i) {
+    double s = g_new[i];
+    for (int j = 0; j < i; ++j) s -= Lc[i * Lmax + j] * Lc[k * Lmax + j];
+    double wi = s / Lc[i * Lmax + i];
+    Lc[k * Lmax + i] = wi;
+    ww += wi * wi;
+  }
+  double piv2 = g_kk - ww;
+  if (!(piv2 > 0.0)) return false;
+  Lc[k * Lmax + k] = std::sqrt(piv2);
+  return true;
+}
+
+void chol_solve(const double* Lc, int Lmax, int k, const double* b, double* x) {
+  double y[64];
+  for (int i = 0; i < k; ++i) {
+    double s = b[i];
+    for (int j = 0; j < i; ++j) s -= Lc[i * Lmax + j] * y[j];
+    y[i] = s / Lc[i * Lmax + i];
+  }
+  for (int i = k - 1; i >= 0; --i) {
+    double s = y[i];
+    for (int j = i + 1; j < k; ++j) s -= Lc[j * Lmax + i] * x[j];
+    x[i] = s / Lc[i * Lmax + i];
+  }
+}
+
+template <typename T>
+inline T dot(const T* a, const T* b, int n) {
+  T s = T(0);
+#pragma omp simd reduction(+ : s)
+  for (int i = 0; i < n; ++i) s += a[i] * b[i];
+  return s;
+}
+
+// ---------------------------------------------------------------------------
+// createPatches (cuda_svd_denoiser.cu:221-256): im2col, patch-major output
+// (the reference's column-major n x N matrix).
+// ---------------------------------------------------------------------------
+template <typename T>
+void extract_patches(const float* img, const Geom& g, T* out) {
+  par_dynamic(g.nx, 1, [&](int64_t b, int64_t e) {
+    for (int64_t ix = b; ix < e; ++ix) {
+      for (int iy = 0; iy < g.ny; ++iy) {
+        int64_t p = ix * g.ny + iy;
+        T* dst = out + p * g.n;
+        int x0 = int(ix) * g.sh, y0 = iy * g.sw;
+        for (int r = 0; r < g.ph; ++r)
+          for (int c = 0; c < g.pw; ++c) dst[r * g.pw + c] = T(img[size_t(y0 + c) * g.W + (x0 + r)]);
+      }
+    }
+  });
+}
+
+// ---------------------------------------------------------------------------
+// initDictionary (cuda_svd_denoiser.cu:261-280) + normalizeDictKernel
+// (:52-63): atoms = patches N/2 .. N/2+K-1, each divided by its 2-norm.
+// With int_norm the squared norm is accumulated as the reference's
+// transform_reduce(..., 0, plus<float>()) does: the accumulator has the type
+// of the int init value, so every partial sum is truncated to int.
+// ---------------------------------------------------------------------------
+template <typename T>
+int init_dictionary(const T* patches, int64_t N, int n, int K, int int_norm, T* D) {
+  int64_t first = N / 2;
+  if (first + K > N) return -1;
+  int bad = 0;
+  for (int k = 0; k < K; ++k) {
+    const T* src = patches + (first + k) * n;
+    T* dst = D + int64_t(k) * n;
+    T norm;
+    if (int_norm) {
+      int acc = 0;
+      for (int i = 0; i < n; ++i) {
+        // volatile keeps the product rounded on its own (no FMA contraction),
+        // as two separate float operations are on the device.
+        float x = float(src[i]);
+        volatile float sq = x * x;
+        float s = float(acc) + sq;
+        acc = int(s);
+      }
+      norm = T(std::sqrt(float(acc)));
+    } else {
+      T s = T(0);
+      for (int i = 0; i < n; ++i) s += src[i] * src[i];
+      norm = std::sqrt(s);
+    }
+    if (!(norm > T(0))) bad = 1;
+    for (int i = 0; i < n; ++i) dst[i] = src[i] / norm;
+  }
+  return bad ? -2 : 0;
+}
+
+// ---------------------------------------------------------------------------
+// CuBlasMatrixOmp::work (cublas_matrix_omp.cu:107-402): per patch,
+//   residual r = y; previous norm = 1 (normsDevice init, :116-117)
+//   for it < L:
+//     skip if previous residual norm < 1e-3                         (:218)
+//     a = argmax_k |d_k . r|, lowest index on ties (cublasIsamax)   (:193-233)
+//     coefficients = least squares of y on the selected atoms       (:269-339)
+//       (the reference uses a pseudo-inverse from gesvda; a Cholesky
+//        solve of the support Gram gives the same least-squares solution)
+//     r = y - D_S gamma; norm = ||r||                               (:352-391)
+// Output: compact codes, idx[p*L + s] (atom or -1) and coef[p*L + s].
+// ---------------------------------------------------------------------------
+template <typename T>
+void omp(const T* Y, int64_t N, int n, const T* D, int K, int L, int32_t* idx, T* coef) {
+  par_dynamic(N, 64, [&](int64_t pb, int64_t pe) {
+    std::vector<T> r(n);
+    std::vector<double> Lc(size_t(L) * L), gnew(L), b(L), gam(L);
+    std::vector<int> S(L);
+    for (int64_t p = pb; p < pe; ++p) {
+      const T* y = Y + p * n;
+      for (int s = 0; s < L; ++s) {
+        idx[p * L + s] = -1;
+        coef[p * L + s] = T(0);
+      }
+      for (int i = 0; i < n; ++i) r[i] = y[i];
+      double prev_norm = 1.0;
+      int k = 0;
+      for (int it = 0; it < L; ++it) {
+        if (prev_norm < 1e-3) break;
+        // correlation and argmax |.|, first index wins ties
+        int a = 0;
+        T best = T(-1);
+        for (int j = 0; j < K; ++j) {
+          T cj = std::fabs(dot(D + int64_t(j) * n, r.data(), n));
+          if (cj > best) {
+            best = cj;
+            a = j;
+          }
+        }
+        bool dup = false;
+        for (int s = 0; s < k; ++s)
+          if (S[s] == a) dup = true;
+        if (dup) break;
+        const T* da = D + int64_t(a) * n;
+        for (int s = 0; s < k; ++s) gnew[s] = double(dot(D + int64_t(S[s]) * n, da, n));
+        double gaa = double(dot(da, da, n));
+        if (!chol_append(Lc.data(), L, k, gnew.data(), gaa)) break;
+        S[k] = a;
+        b[k] = double(dot(da, y, n));
+        ++k;
+        chol_solve(Lc.data(), L, k, b.data(), gam.data());
+        for (int i = 0; i < n; ++i) r[i] = y[i];
+        for (int s = 0; s < k; ++s) {
+          const T* ds = D + int64_t(S[s]) * n;
+          T gs = T(gam[s]);
+          for (int i = 0; i < n; ++i) r[i] -= gs * ds[i];
+        }
+        double nrm = 0.0;
+        for (int i = 0; i < n; ++i) nrm += double(r[i]) * double(r[i]);
+        prev_norm = std::sqrt(nrm);
+      }
+      for (int s = 0; s < k; ++s) {
+        idx[p * L + s] = S[s];
+        coef[p * L + s] = T(gam[s]);
+      }
+    }
+  });
+}
+
+// ---------------------------------------------------------------------------
+// CudaKSvdDenoiser::updateDictionary (cuda_svd_denoiser.cu:285-362).
+// Omega_j = patches with a nonzero coefficient on atom j, in ascending patch
+// order, found once before the sweep (findRelevantIndicesKernel :36-50,
+// launched at :298).  Atoms are visited in order; unused atoms are skipped
+// (:311-312).  For atom j:
+//   E[:, t] = y_p - sum_{s != j} x_{s,p} d_s   for the t-th patch p of Omega_j
+//   (u, sigma, v) = top singular triplet of E    (gesvdj, :328-332)
+//   d_j <- u;  x_{j,p_t} <- sigma v_t             (:343-358)
+// sigma v_t = u . E[:, t], so the coefficients are the projections on u.
+// The sign of u is fixed so that u . d_j(old) >= 0 (the reference's sign
+// comes from cuSOLVER; D X is invariant under the sign).
+// With q1_cap, columns t >= 1024 of E are zero (see the file header).
+// ---------------------------------------------------------------------------
+template <typename T>
+int update_dictionary(const T* Y, int64_t N, int n, T* D, int K, int L, const int32_t* idx, T* coef,
+                      int q1_cap) {
+  // CSR of atom -> (patch, slot), ascending patch order
+  std::vector<int64_t> cnt(K + 1, 0);
+  for (int64_t p = 0; p < N; ++p)
+    for (int s = 0; s < L; ++s) {
+      int a = idx[p * L + s];
+      if (a >= 0 && coef[p * L + s] != T(0)) cnt[a + 1]++;
+    }
+  for (int k = 0; k < K; ++k) cnt[k + 1] += cnt[k];
+  std::vector<int64_t> ent(cnt[K]);
+  {
+    std::vector<int64_t> pos(cnt.begin(), cnt.end() - 1);
+    for (int64_t p = 0; p < N; ++p)
+      for (int s = 0; s < L; ++s) {
+        int a = idx[p * L + s];
+        if (a >= 0 && coef[p * L + s] != T(0)) ent[pos[a]++] = p * L + s;
+      }
+  }
+  int nthreads = num_threads();
+  std::vector<double> G(size_t(n) * n);
+  std::vector<std::vector<double>> Gpart(nthreads, std::vector<double>(size_t(n) * n));
+  std::vector<double> u(n);
+  for (int j = 0; j < K; ++j) {
+    int64_t beg = cnt[j], end = cnt[j + 1];
+    int64_t c = end - beg;
+    if (c < 1) continue;
+    int64_t c_eff = (q1_cap && c > 1024) ? 1024 : c;
+    // G = E E^T over the effective columns (static split: fixed summation order)
+    int T_used = int(std::min<int64_t>(nthreads, std::max<int64_t>(1, c_eff / 16)));
+    par_static(c_eff, T_used, [&](int tid, int64_t tb, int64_t te) {
+      std::vector<double>& Gp = Gpart[tid];
+      std::fill(Gp.begin(), Gp.end(), 0.0);
+      std::vector<T> e(n);
+      for (int64_t t = tb; t < te; ++t) {
+        int64_t es = ent[beg + t];
+        int64_t p = es / L;
+        int slot = int(es % L);
+        const T* y = Y + p * n;
+        for (int i = 0; i < n; ++i) e[i] = y[i];
+        for (int s = 0; s < L; ++s) {
+          int a = idx[p * L + s];
+          if (s == slot || a < 0) continue;
+          T x = coef[p * L + s];
+          const T* da = D + int64_t(a) * n;
+          for (int i = 0; i < n; ++i) e[i] -= x * da[i];
+        }
+        for (int i = 0; i < n; ++i) {
+          double ei = double(e[i]);
+          double* row = Gp.data() + size_t(i) * n;
+          for (int k2 = 0; k2 <= i; ++k2) row[k2] += ei * double(e[k2]);
+        }
+      }
+    });
+    std::fill(G.begin(), G.end(), 0.0);
+    for (int t = 0; t < T_used; ++t)
+      for (size_t q = 0; q < G.size(); ++q) G[q] += Gpart[t][q];
+    for (int i = 0; i < n; ++i)
+      for (int k2 = 0; k2 < i; ++k2) G[size_t(k2) * n + i] = G[size_t(i) * n + k2];
+    sym_top_eig(G, n, u.data());
+    T* dj = D + int64_t(j) * n;
+    double sgn = 0.0;
+    for (int i = 0; i < n; ++i) sgn += u[i] * double(dj[i]);
+    if (sgn < 0.0)
+      for (int i = 0; i < n; ++i) u[i] = -u[i];
+    // coefficients x_{j,p} = u . e_p (e_p built with the OLD atom set, which
+    // does not involve d_j itself), zero beyond the cap
+    par_dynamic(c, 256, [&](int64_t tb, int64_t te) {
+      std::vector<T> e(n);
+      for (int64_t t = tb; t < te; ++t) {
+        int64_t es = ent[beg + t];
+        if (t >= c_eff) {
+          coef[es] = T(0);
+          continue;
+        }
+        int64_t p = es / L;
+        int slot = int(es % L);
+        const T* y = Y + p * n;
+        for (int i = 0; i < n; ++i) e[i] = y[i];
+        for (int s = 0; s < L; ++s) {
+          int a = idx[p * L + s];
+          if (s == slot || a < 0) continue;
+          T x = coef[p * L + s];
+          const T* da = D + int64_t(a) * n;
+          for (int i = 0; i < n; ++i) e[i] -= x * da[i];
+        }
+        double acc = 0.0;
+        for (int i = 0; i < n; ++i) acc += u[i] * double(e[i]);
+        coef[es] = T(acc);
+      }
+    });
+    for (int i = 0; i < n; ++i) dj[i] = T(u[i]);
+  }
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// createImage (cuda_svd_denoiser.cu:413-498): patches D X, overlap-add with
+// unit block weights, lambda = |sqrt(sum (img/w - y)^2 / (sigma2 * P)) - 1|,
+// out = (lambda y + img) / (lambda + w), exp2 for speckle (:483-484).
+// y is the (log-domain, for speckle) noisy input.
+// ---------------------------------------------------------------------------
+template <typename T>
+void build_image(const float* noisy, const Geom& g, const T* D, int K, int L, const int32_t* idx,
+                 const T* coef, double sigma2, int speckle, float* out, double* lambda_out) {
+  (void)K;
+  size_t P = size_t(g.W) * g.H;
+  std::vector<double> acc(P, 0.0), w(P, 0.0);
+  std::vector<T> xh(g.n);
+  for (int ix = 0; ix < g.nx; ++ix)
+    for (int iy = 0; iy < g.ny; ++iy) {
+      int64_t p = int64_t(ix) * g.ny + iy;
+      for (int i = 0; i < g.n; ++i) xh[i] = T(0);
+      for (int s = 0; s < L; ++s) {
+        int a = idx[p * L + s];
+        if (a < 0) continue;
+        T x = coef[p * L + s];
+        const T* da = D + int64_t(a) * g.n;
+        for (int i = 0; i < g.n; ++i) xh[i] += x * da[i];
+      }
+      int x0 = ix * g.sh, y0 = iy * g.sw;
+      for (int r = 0; r < g.ph; ++r)
+        for (int c = 0; c < g.pw; ++c) {
+          size_t q = size_t(y0 + c) * g.W + (x0 + r);
+          acc[q] += double(xh[r * g.pw + c]);
+          w[q] += 1.0;
+        }
+    }
+  double ssum = 0.0;
+  for (size_t q = 0; q < P; ++q)
+    if (w[q] > 0.0) {
+      double dlt = acc[q] / w[q] - double(noisy[q]);
+      ssum += dlt * dlt;
+    }
+  double d = ssum / (sigma2 * double(P));
+  double lam = std::fabs(std::sqrt(d) - 1.0);
+  if (lambda_out) *lambda_out = lam;
+  for (size_t q = 0; q < P; ++q) {
+    double v = (w[q] > 0.0) ? (lam * double(noisy[q]) + acc[q]) / (lam + w[q]) : double(noisy[q]);
+    if (speckle) v = std::exp2(v);
+    out[q] = float(v);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+void ko_set_threads(int t) { g_threads = t > 0 ? t : 0; }
+
+int ko_max_threads(void) { return num_threads(); }
+
+int64_t ko_num_patches(int W, int H, int pw, int ph, int sw, int sh) {
+  Geom g;
+  if (!make_geom(W, H, pw, ph, sw, sh, &g)) return -1;
+  return g.N;
+}
+
+int ko_extract_patches(const float* img, int W, int H, int pw, int ph, int sw, int sh, float* out) {
+  Geom g;
+  if (!make_geom(W, H, pw, ph, sw, sh, &g)) return -1;
+  extract_patches<float>(img, g, out);
+  return 0;
+}
+
+int ko_init_dictionary_f32(const float* P, int64_t N, int n, int K, int int_norm, float* D) {
+  return init_dictionary<float>(P, N, n, K, int_norm, D);
+}
+int ko_init_dictionary_f64(const double* P, int64_t N, int n, int K, int int_norm, double* D) {
+  return init_dictionary<double>(P, N, n, K, int_norm, D);
+}
+
+int ko_omp_f32(const float* Y, int64_t N, int n, const float* D, int K, int L, int32_t* idx, float* coef) {
+  if (L < 1 || L > 64) return -1;
+  omp<float>(Y, N, n, D, K, L, idx, coef);
+  return 0;
+}
+int ko_omp_f64(const double* Y, int64_t N, int n, const double* D, int K, int L, int32_t* idx, double* coef) {
+  if (L < 1 || L > 64) return -1;
+  omp<double>(Y, N, n, D, K, L, idx, coef);
+  return 0;
+}
+
+int ko_update_f32(const float* Y, int64_t N, int n, float* D, int K, int L, const int32_t* idx, float* coef,
+                  int q1_cap) {
+  return update_dictionary<float>(Y, N, n, D, K, L, idx, coef, q1_cap);
+}
+int ko_update_f64(const double* Y, int64_t N, int n, double* D, int K, int L, const int32_t* idx,
+                  double* coef, int q1_cap) {
+  return update_dictionary<double>(Y, N, n, D, K, L, idx, coef, q1_cap);
+}
+
+int ko_build_image_f32(const float* noisy, int W, int H, int pw, int ph, int sw, int sh, const float* D, int K,
+                       int L, const int32_t* idx, const float* coef, double sigma2, int speckle, float* out,
+                       double* lambda_out) {
+  Geom g;
+  if (!make_geom(W, H, pw, ph, sw, sh, &g)) return -1;
+  build_image<float>(noisy, g, D, K, L, idx, coef, sigma2, speckle, out, lambda_out);
+  return 0;
+}
+int ko_build_image_f64(const float* noisy, int W, int H, int pw, int ph, int sw, int sh, const double* D, int K,
+                       int L, const int32_t* idx, const double* coef, double sigma2, int speckle, float* out,
+                       double* lambda_out) {
+  Geom g;
+  if (!make_geom(W, H, pw, ph, sw, sh, &g)) return -1;
+  build_image<double>(noisy, g, D, K, L, idx, coef, sigma2, speckle, out, lambda_out);
+  return 0;
+}
+
+// Top eigenpair of a symmetric matrix (exposed for tests of the solver).
+double ko_sym_top_eig(const double* A, int n, double* u) {
+  std::vector<double> M(A, A + size_t(n) * n);
+  return sym_top_eig(M, n, u);
+}
+
+}  // extern "C"

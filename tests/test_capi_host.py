@@ -1,0 +1,77 @@
+"""Host-side checks of the C ABI: the library loads, exports every declared
+symbol, and its host-only entry points behave (no GPU work)."""
+
+import ctypes
+
+import pytest
+
+
+def test_exports_every_declared_symbol(built_lib, ksvd):
+    names = ksvd.declared_symbols()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(built_lib, n)]
+    assert not missing, missing
+
+
+def test_abi_version(built_lib):
+    assert built_lib.ksvd_abi_version() == 1
+
+
+def test_params_default_match_reference(ksvd, built_lib):
+    # denoisingLib.h:44-56
+    p = ksvd.default_params()
+    assert (p.patch_width_dim, p.patch_height_dim) == (8, 8)
+    assert (p.sliding_width, p.sliding_height) == (2, 2)
+    assert (p.atoms, p.ksvd_iter, p.omp_iter) == (256, 10, 5)
+    assert (p.sub_image_width_dim, p.sub_image_height_dim) == (0, 0)
+    assert p.bw == 1 and p.speckle == 0 and p.min_omp_iter_batch == 0
+    assert p.type == ksvd.CUDA_K_SM100A
+    assert p.compat == ksvd.COMPAT_REFERENCE
+
+
+def test_type_map(ksvd, built_lib):
+    # DenoiserTypeMap (denoisingLib.h:23-31); unknown names map to 0 like
+    # std::map::operator[]
+    assert ksvd.type_from_string("CUDA_K_GESVD") == (0, True)
+    assert ksvd.type_from_string("CUDA_K_GESVDJ") == (1, True)
+    assert ksvd.type_from_string("CUDA_K_GESVDA") == (2, True)
+    assert ksvd.type_from_string("CUDA_K_SM100A") == (3, True)
+    assert ksvd.type_from_string("nonsense") == (0, False)
+    assert built_lib.ksvd_type_name(1) == b"CUDA_K_GESVDJ"
+
+
+def test_num_patches(ksvd, built_lib):
+    p = ksvd.make_params(patch_width_dim=12, patch_height_dim=12, sliding_width=3, sliding_height=3)
+    assert ksvd.num_patches(p, 512, 512) == 167 * 167
+    assert ksvd.num_patches(p, 2048, 2048) == 679 * 679
+    assert ksvd.num_patches(p, 11, 512) == -1
+
+
+def test_status_strings(built_lib):
+    assert built_lib.ksvd_status_string(0) == b"ok"
+    assert built_lib.ksvd_status_string(-1) == b"image loading failed"
+    assert built_lib.ksvd_status_string(-2) == b"denoising failed"
+    assert built_lib.ksvd_status_string(-3) == b"image saving failed"
+
+
+def test_create_rejects_bad_params(ksvd, built_lib):
+    for kw in (dict(atoms=0), dict(omp_iter=0), dict(omp_iter=33), dict(sliding_width=0), dict(type=7)):
+        p = ksvd.make_params(**kw)
+        h = ctypes.c_void_p()
+        assert built_lib.ksvd_create(ctypes.byref(p), ctypes.byref(h)) == ksvd.ERR_INVALID
+
+
+def test_create_without_gpu_reports_no_device(ksvd, built_lib):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    p = ksvd.default_params()
+    h = ctypes.c_void_p()
+    assert built_lib.ksvd_create(ctypes.byref(p), ctypes.byref(h)) == ksvd.ERR_NO_DEVICE
+    with pytest.raises(ksvd.KsvdError):
+        ksvd.Context()
+
+
+def test_null_context_is_rejected(built_lib, ksvd):
+    assert built_lib.ksvd_omp(None, None, 0, None, None, None) == ksvd.ERR_INVALID
+    assert built_lib.ksvd_last_error(None) == b"null context"

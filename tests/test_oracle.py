@@ -1,0 +1,292 @@
+"""The CPU oracle against independent restatements (numpy / LAPACK) and
+hand-computed cases.  No GPU needed."""
+
+import numpy as np
+import pytest
+
+
+# ---------------------------------------------------------------------------
+# independent numpy restatements of the reference steps (small sizes only)
+# ---------------------------------------------------------------------------
+def np_patches(img, pw, ph, sw, sh):
+    """createPatches, cuda_svd_denoiser.cu:221-256: outer x (step sh, extent
+    ph), inner y (step sw, extent pw), element r*pw + c = pixel (x+r, y+c)."""
+    H, W = img.shape
+    out = []
+    for x in range(0, W - ph + 1, sh):
+        for y in range(0, H - pw + 1, sw):
+            out.append(img[y:y + pw, x:x + ph].T.reshape(-1))
+    return np.array(out, np.float32)
+
+
+def np_omp(Y, D, L):
+    """OMP by explicit least squares (numpy lstsq)."""
+    N = Y.shape[0]
+    idx = -np.ones((N, L), np.int32)
+    coef = np.zeros((N, L))
+    for p in range(N):
+        y = Y[p].astype(np.float64)
+        r = y.copy()
+        S = []
+        prev = 1.0
+        g = np.zeros(0)
+        for _ in range(L):
+            if prev < 1e-3:
+                break
+            c = np.abs(D @ r)
+            a = int(np.argmax(c))  # first index of the maximum
+            if a in S:
+                break
+            S.append(a)
+            g, *_ = np.linalg.lstsq(D[S].T, y, rcond=None)
+            r = y - D[S].T @ g
+            prev = np.linalg.norm(r)
+        idx[p, :len(S)] = S
+        coef[p, :len(S)] = g if S else []
+    return idx, coef
+
+
+def np_update(Y, D, idx, coef, q1_cap):
+    """updateDictionary with numpy's SVD for the top singular triplet."""
+    D = D.copy()
+    coef = coef.copy()
+    N, L = idx.shape
+    K = D.shape[0]
+    supp = [[] for _ in range(K)]
+    for p in range(N):
+        for s in range(L):
+            if idx[p, s] >= 0 and coef[p, s] != 0:
+                supp[idx[p, s]].append((p, s))
+    for j in range(K):
+        ent = supp[j]
+        if not ent:
+            continue
+        ceff = min(len(ent), 1024) if q1_cap else len(ent)
+        E = np.zeros((D.shape[1], len(ent)))
+        for t, (p, s) in enumerate(ent[:ceff]):
+            e = Y[p].astype(np.float64).copy()
+            for s2 in range(L):
+                if s2 != s and idx[p, s2] >= 0:
+                    e -= coef[p, s2] * D[idx[p, s2]]
+            E[:, t] = e
+        U, S, Vt = np.linalg.svd(E, full_matrices=False)
+        u = U[:, 0]
+        v = S[0] * Vt[0]
+        if u @ D[j] < 0:
+            u, v = -u, -v
+        D[j] = u
+        for t, (p, s) in enumerate(ent):
+            coef[p, s] = v[t]
+    return D, coef
+
+
+def recon_err(Y, D, idx, coef):
+    rec = np.zeros(Y.shape)
+    for s in range(idx.shape[1]):
+        m = idx[:, s] >= 0
+        rec[m] += coef[m, s:s + 1] * D[idx[m, s]]
+    return np.linalg.norm(Y - rec)
+
+
+@pytest.fixture(scope="module")
+def small_case(synth, oracle):
+    clean = synth.clean_image(48, 7)
+    noisy = synth.add_gaussian(clean, 20.0, 7)
+    Y = oracle.extract_patches(noisy, 8, 8, 2, 2)
+    return clean, noisy, Y
+
+
+# ---------------------------------------------------------------------------
+def test_sym_top_eig_matches_lapack(oracle):
+    r = np.random.default_rng(0)
+    for n in (1, 2, 3, 7, 64, 144, 160):
+        X = r.normal(size=(n, 2 * n + 3))
+        A = X @ X.T
+        lam, u = oracle.sym_top_eig(A)
+        w, V = np.linalg.eigh(A)
+        assert abs(lam - w[-1]) <= 1e-12 * abs(w[-1])
+        v = V[:, -1]
+        assert min(np.abs(u - v).max(), np.abs(u + v).max()) < 1e-9
+
+
+def test_extract_patches_geometry(oracle):
+    img = np.arange(7 * 9, dtype=np.float32).reshape(7, 9)  # H=7, W=9
+    for (pw, ph, sw, sh) in [(2, 2, 1, 1), (3, 2, 2, 1), (2, 3, 1, 2), (4, 4, 3, 3)]:
+        got = oracle.extract_patches(img, pw, ph, sw, sh)
+        np.testing.assert_array_equal(got, np_patches(img, pw, ph, sw, sh))
+    # patch 0 of a 2x2/stride-1 walk: x=0..1, y=0..1, element r*pw+c = (x=r, y=c)
+    p = oracle.extract_patches(img, 2, 2, 1, 1)
+    np.testing.assert_array_equal(p[0], [img[0, 0], img[1, 0], img[0, 1], img[1, 1]])
+    # the second patch moves along y (inner index), the (ny+1)-th along x
+    np.testing.assert_array_equal(p[1], [img[1, 0], img[2, 0], img[1, 1], img[2, 1]])
+    ny = 7 - 2 + 1
+    np.testing.assert_array_equal(p[ny], [img[0, 1], img[1, 1], img[0, 2], img[1, 2]])
+
+
+def test_num_patches(oracle):
+    assert oracle.num_patches(512, 512, 12, 12, 3, 3) == 167 * 167
+    assert oracle.num_patches(2048, 2048, 12, 12, 3, 3) == 679 * 679
+    assert oracle.num_patches(4096, 4096, 16, 16, 2, 2) == 2041 * 2041
+    assert oracle.num_patches(8, 8, 9, 9, 1, 1) == -1
+
+
+def test_init_dictionary_int_norm(oracle, small_case):
+    _, _, Y = small_case
+    K = 16
+    N = Y.shape[0]
+    D = oracle.init_dictionary(Y, K, int_norm=True, dtype=np.float32)
+    # restate the truncating accumulation in numpy float32
+    for k in range(K):
+        src = Y[N // 2 + k]
+        acc = 0
+        for x in src:
+            acc = int(np.float32(np.float32(acc) + np.float32(x) * np.float32(x)))
+        norm = np.sqrt(np.float32(acc))
+        np.testing.assert_array_equal(D[k], (src / norm).astype(np.float32))
+    Dx = oracle.init_dictionary(Y, K, int_norm=False, dtype=np.float64)
+    np.testing.assert_allclose(np.linalg.norm(Dx, axis=1), 1.0, rtol=1e-12)
+    # the int accumulator drops fractions, so those atoms are slightly longer
+    assert np.all(np.linalg.norm(D.astype(np.float64), axis=1) >= 1.0 - 1e-6)
+
+
+def test_init_dictionary_errors(oracle):
+    Y = np.ones((10, 4), np.float32)
+    with pytest.raises(ValueError):
+        oracle.init_dictionary(Y, 6)
+    Y[5:] = 0
+    with pytest.raises(FloatingPointError):
+        oracle.init_dictionary(Y, 2)
+
+
+def test_omp_matches_numpy_lstsq(oracle, small_case):
+    _, _, Y = small_case
+    D = oracle.init_dictionary(Y, 24, int_norm=False)
+    idx, coef = oracle.omp(Y, D, 5)
+    idx2, coef2 = np_omp(Y, D, 5)
+    agree = np.all(idx == idx2, axis=1)
+    assert agree.mean() > 0.999
+    np.testing.assert_allclose(coef[agree], coef2[agree], rtol=1e-8, atol=1e-8)
+
+
+def test_omp_residual_orthogonal(oracle, small_case):
+    _, _, Y = small_case
+    D = oracle.init_dictionary(Y, 24, int_norm=False)
+    idx, coef = oracle.omp(Y, D, 5)
+    for p in range(0, Y.shape[0], 37):
+        S = idx[p][idx[p] >= 0]
+        r = Y[p] - coef[p, :len(S)] @ D[S]
+        assert np.abs(D[S] @ r).max() < 1e-9 * np.linalg.norm(Y[p])
+
+
+def test_omp_tie_break_and_stop(oracle):
+    # two identical atoms: argmax must take the lower index; then the exact
+    # representation stops the pursuit (residual norm < 1e-3)
+    D = np.zeros((4, 4))
+    D[0] = [1, 0, 0, 0]
+    D[1] = [0, 1, 0, 0]
+    D[2] = [0, 1, 0, 0]
+    D[3] = [0, 0, 1, 0]
+    Y = np.array([[0, 3.0, 0, 0], [0, 0, 0, 0]])
+    idx, coef = oracle.omp(Y, D, 3)
+    assert list(idx[0]) == [1, -1, -1]
+    assert coef[0, 0] == pytest.approx(3.0)
+    # zero patch: the first step runs (initial norm 1), picks atom 0 with a
+    # zero coefficient, then stops
+    assert list(idx[1]) == [0, -1, -1]
+    assert coef[1, 0] == 0.0
+
+
+def test_omp_dependent_atom_stops(oracle):
+    # y needs atoms 0 and 1; atom 2 = atom 0 duplicate never enters
+    D = np.array([[1.0, 0, 0], [0, 1.0, 0], [1.0, 0, 0]])
+    Y = np.array([[2.0, 1.0, 0.5]])
+    idx, coef = oracle.omp(Y, D, 3)
+    assert list(idx[0]) == [0, 1, -1]
+
+
+def test_update_matches_numpy_svd(oracle, small_case):
+    _, _, Y = small_case
+    D = oracle.init_dictionary(Y, 24, int_norm=False)
+    idx, coef = oracle.omp(Y, D, 4)
+    for q1 in (False, True):
+        D1, c1 = oracle.update_dictionary(Y, D, idx, coef, q1_cap=q1)
+        D2, c2 = np_update(Y, D, idx, coef, q1)
+        np.testing.assert_allclose(D1, D2, atol=1e-9)
+        np.testing.assert_allclose(c1, c2, rtol=1e-7, atol=1e-7)
+        assert recon_err(Y, D1, idx, c1) < recon_err(Y, D, idx, coef)
+
+
+def test_update_q1_cap_zeroes_tail(oracle, synth):
+    clean = synth.clean_image(96, 3)
+    noisy = synth.add_gaussian(clean, 10.0, 3)
+    Y = oracle.extract_patches(noisy, 4, 4, 1, 1)  # 93^2 = 8649 patches
+    D = oracle.init_dictionary(Y, 8, int_norm=False)
+    idx, coef = oracle.omp(Y, D, 2)
+    counts = np.bincount(idx[idx >= 0], minlength=8)
+    j = int(np.argmax(counts))
+    assert counts[j] > 1024
+    D1, c1 = oracle.update_dictionary(Y, D, idx, coef, q1_cap=True)
+    D2, c2 = np_update(Y, D, idx, coef, True)
+    np.testing.assert_allclose(D1, D2, atol=1e-9)
+    np.testing.assert_allclose(c1, c2, rtol=1e-7, atol=1e-7)
+    ps, ss = np.nonzero((idx == j) & (coef != 0))
+    order = np.argsort(ps)
+    tail = c1[ps[order][1024:], ss[order][1024:]]
+    assert np.all(tail == 0.0)
+
+
+def test_build_image_matches_numpy(oracle, small_case):
+    clean, noisy, Y = small_case
+    D = oracle.init_dictionary(Y, 24, int_norm=False)
+    idx, coef = oracle.omp(Y, D, 5)
+    out, lam = oracle.build_image(noisy, 8, 8, 2, 2, D, idx, coef, 400.0)
+    H, W = noisy.shape
+    acc = np.zeros((H, W))
+    w = np.zeros((H, W))
+    p = 0
+    for x in range(0, W - 8 + 1, 2):
+        for y in range(0, H - 8 + 1, 2):
+            S = idx[p][idx[p] >= 0]
+            xh = (coef[p, :len(S)] @ D[S]).reshape(8, 8)  # [r][c] = (x+r, y+c)
+            acc[y:y + 8, x:x + 8] += xh.T
+            w[y:y + 8, x:x + 8] += 1
+            p += 1
+    cov = w > 0
+    d = np.sum((acc[cov] / w[cov] - noisy[cov]) ** 2) / (400.0 * H * W)
+    lam2 = abs(np.sqrt(d) - 1)
+    assert lam == pytest.approx(lam2, rel=1e-12)
+    ref = np.where(cov, (lam2 * noisy + acc) / (lam2 + w), noisy)
+    np.testing.assert_allclose(out, ref, rtol=1e-6, atol=1e-4)
+
+
+def test_ksvd_denoise_improves_psnr(oracle, synth):
+    clean = synth.clean_image(64, 11)
+    noisy = synth.add_gaussian(clean, 20.0, 11)
+    out, info = oracle.ksvd_denoise(noisy, 400.0, pw=8, ph=8, sw=2, sh=2, atoms=32, ksvd_iter=3)
+    assert synth.psnr(clean, out) > synth.psnr(clean, noisy) + 1.5
+
+
+def test_speckle_roundtrip(oracle, synth):
+    clean = synth.clean_image(48, 5) + 1.0
+    noisy = synth.add_speckle(clean, 4.0, 5)
+    out, _ = oracle.ksvd_denoise(noisy, 0.3, pw=8, ph=8, sw=4, sh=4, atoms=16, ksvd_iter=1, speckle=True)
+    assert np.all(np.isfinite(out)) and out.min() > 0
+
+
+def test_golden_fixtures(oracle):
+    """Fixtures in tests/golden/ (see tests/golden/README.md) replayed on the
+    FP32 oracle."""
+    from pathlib import Path
+    gdir = Path(__file__).parent / "golden"
+    files = sorted(gdir.glob("*.npz"))
+    if not files:
+        pytest.skip("no golden fixtures committed")
+    for f in files:
+        z = np.load(f)
+        kind = str(z["kind"])
+        if kind == "omp":
+            idx, coef = oracle.omp(z["patches"], z["dict"], int(z["L"]), dtype=np.float32)
+            agree = np.mean(np.all(idx == z["idx"], axis=1))
+            assert agree >= float(z["min_agree"]), (f.name, agree)
+            m = np.all(idx == z["idx"], axis=1)
+            np.testing.assert_allclose(coef[m], z["coef"][m], rtol=float(z["rtol"]), atol=float(z["atol"]))
