@@ -276,6 +276,7 @@ def main():
     ms_total = ev0.elapsed_time(ev1)
     gpu_launches = ctx.launch_count() - launches0
     fam = {f: ctx.profile_read(f) for f in ("gram", "omp", "csr", "update")}
+    phases = ctx.profile_phases()
     ctx.profile(False)
     ms_step = ms_total / args.steps
     if dist:
@@ -351,6 +352,10 @@ def main():
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
                          "algorithmic_bytes_per_patch": bytes_per_patch, "avg_launch_ms": avg_ms},
             "kernel_ms_per_step": {f: fam[f][0] / max(args.steps, 1) for f in fam},
+            "phase_ms_per_step": {
+                name: phases[i] / max(args.steps, 1) for i, name in (
+                    (0, "upd_gram"), (1, "upd_wait1"), (2, "upd_sum"), (3, "upd_wait2"), (4, "upd_power"),
+                    (5, "upd_coef"), (6, "upd_wait3"), (8, "omp_corr"), (9, "omp_ls"), (10, "omp_io"))},
             "quality": {"psnr_noisy": psnr_noisy, "psnr_denoised": psnr_out,
                         "power_iters_last_sweep": st.power_iters, "atoms_updated_last_sweep": st.atoms_updated},
             "clocks": clocks.summary(),

@@ -245,6 +245,8 @@ ksvd_status ksvd_create(const ksvd_params* p, ksvd_ctx** out) {
       cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaMalloc(&c->d_flags, sizeof(ksvd::GridBarrier)) != cudaSuccess ||
       cudaMalloc(&c->d_stats, sizeof(ksvd::DevStats)) != cudaSuccess ||
+      cudaMalloc(&c->d_phase, sizeof(ksvd::DevStats)) != cudaSuccess ||
+      cudaMemset(c->d_phase, 0, sizeof(ksvd::DevStats)) != cudaSuccess ||
       cudaMemset(c->d_flags, 0, sizeof(ksvd::GridBarrier)) != cudaSuccess ||
       cudaMemset(c->d_stats, 0, sizeof(ksvd::DevStats)) != cudaSuccess) {
     cudaGetLastError();
@@ -270,6 +272,7 @@ void ksvd_destroy(ksvd_ctx* c) {
   for (auto e : c->event_pool) cudaEventDestroy(e);
   if (c->d_flags) cudaFree(c->d_flags);
   if (c->d_stats) cudaFree(c->d_stats);
+  if (c->d_phase) cudaFree(c->d_phase);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
 }
@@ -293,6 +296,7 @@ ksvd_status ksvd_profile_enable(ksvd_ctx* c, int enable) {
 ksvd_status ksvd_profile_reset(ksvd_ctx* c) {
   if (!c) return KSVD_ERR_INVALID;
   cudaStreamSynchronize(c->stream);
+  cudaMemset(c->d_phase, 0, sizeof(ksvd::DevStats));
   for (auto& kv : c->families) {
     for (auto& pr : kv.second.pending) {
       c->event_pool.push_back(pr.first);
@@ -330,6 +334,16 @@ ksvd_status ksvd_profile_read(ksvd_ctx* c, const char* family, double* total_ms,
 }
 
 int64_t ksvd_launch_count(const ksvd_ctx* c) { return c ? c->launch_count : 0; }
+
+ksvd_status ksvd_profile_phases(ksvd_ctx* c, double* ms_out, int count) {
+  if (!c || !ms_out || count < 1) return KSVD_ERR_INVALID;
+  KSVD_TRY(check_ctx(c));
+  ksvd::DevStats h{};
+  KSVD_CU(c, cudaStreamSynchronize(c->stream), "profile sync");
+  KSVD_CU(c, cudaMemcpy(&h, c->d_phase, sizeof(h), cudaMemcpyDeviceToHost), "phase timers");
+  for (int i = 0; i < count; ++i) ms_out[i] = (i < 16) ? double(h.phase_ns[i]) * 1e-6 : 0.0;
+  return KSVD_OK;
+}
 
 // ---------------------------------------------------------------------------
 // Stage entry points
@@ -370,7 +384,9 @@ static ksvd_status omp_impl(ksvd_ctx* c, const float* d_patches, int64_t N, cons
     KSVD_CU(c, ksvd::launch_gram_f64(d_dict, K, n, gram, c->stream), "gram");
   }
   Prof pr(c, "omp", 1);
-  KSVD_CU(c, ksvd::launch_omp_fp32(d_patches, N, n, d_dict, gram, K, L, d_idx, d_coef, c->num_sms, c->stream),
+  KSVD_CU(c,
+          ksvd::launch_omp_fp32(d_patches, N, n, d_dict, gram, K, L, d_idx, d_coef, c->num_sms,
+                                c->profiling ? c->d_phase : nullptr, c->stream),
           "omp");
   return KSVD_OK;
 }
@@ -391,7 +407,7 @@ static ksvd_status update_impl(ksvd_ctx* c, const float* d_patches, int64_t N, f
   KSVD_TRY(wsT(c, "csr_counts", size_t(w.nchunks) * K, &w.chunk_counts));
   KSVD_TRY(wsT(c, "csr_atom_ptr", size_t(2) * K + 1, &w.atom_ptr));
   KSVD_TRY(wsT(c, "csr_entries", size_t(N) * L, &w.entries));
-  const int grid = ksvd::update_grid_size(n, c->num_sms);
+  const int grid = ksvd::update_grid_size(n, K, L, c->num_sms);
   if (grid < 1) return fail(c, KSVD_ERR_CUDA, "update kernel cannot be made co-resident");
   float *gpart = nullptr, *gsum = nullptr;
   KSVD_TRY(wsT(c, "upd_gpart", size_t(grid) * n * n, &gpart));
@@ -407,6 +423,10 @@ static ksvd_status update_impl(ksvd_ctx* c, const float* d_patches, int64_t N, f
                               (c->p.compat & KSVD_COMPAT_Q1_CAP) ? 1 : 0, gpart, gsum, c->d_flags, c->d_stats,
                               grid, c->stream),
           "update");
+  if (c->profiling) {
+    // fold this sweep's phase timers into the profiling accumulator
+    KSVD_CU(c, ksvd::launch_accumulate_phases(c->d_stats, c->d_phase, c->stream), "phase timers");
+  }
   return KSVD_OK;
 }
 

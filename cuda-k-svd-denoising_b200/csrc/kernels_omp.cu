@@ -78,7 +78,7 @@ __device__ __forceinline__ bool better(float v1, int i1, float v2, int i2) {
 __global__ void __launch_bounds__(kOmpThreads, 1)
     omp_fp32_kernel(const float* __restrict__ Y, int64_t N, int n, const float* __restrict__ D,
                     const double* __restrict__ Gram, int K, int L, int32_t* __restrict__ idx_out,
-                    float* __restrict__ coef_out, int64_t ntiles) {
+                    float* __restrict__ coef_out, int64_t ntiles, DevStats* stats) {
   extern __shared__ __align__(16) unsigned char smem[];
   const OmpLayout lo = omp_layout(n, K, L);
   float* Dk = reinterpret_cast<float*>(smem + lo.off_dk);
@@ -112,6 +112,15 @@ __global__ void __launch_bounds__(kOmpThreads, 1)
   __syncthreads();
 
   const int ag = tid >> 3, pg = tid & 7;  // atom group (32), patch group (8)
+  const bool timer = (blockIdx.x == 0 && tid == 0 && stats != nullptr);
+  unsigned long long tmark = timer ? globaltimer_ns() : 0ull;
+  auto lap = [&](int slot) {
+    if (timer) {
+      const unsigned long long t = globaltimer_ns();
+      stats->phase_ns[slot] += t - tmark;
+      tmark = t;
+    }
+  };
 
   for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int64_t p0 = tile * kTP;
@@ -128,6 +137,7 @@ __global__ void __launch_bounds__(kOmpThreads, 1)
       done[tid] = (tid >= np);
     }
     __syncthreads();
+    lap(10);
 
     for (int step = 0; step < L; ++step) {
       const int active = (tid < kTP) ? !done[tid] : 0;
@@ -209,6 +219,7 @@ __global__ void __launch_bounds__(kOmpThreads, 1)
         sel[tid] = (i < K) ? i : 0;
       }
       __syncthreads();
+      lap(8);
 
       // ---- least squares on the grown support, residual, norm -------------
       for (int q = 0; q < kTP / 8; ++q) {
@@ -279,6 +290,7 @@ __global__ void __launch_bounds__(kOmpThreads, 1)
         if (lane == 0 && sqrtf(nrm) < 1e-3f) done[p] = 1;
       }
       __syncthreads();
+      lap(9);
     }
 
     // ---- compact codes ------------------------------------------------------
@@ -289,6 +301,7 @@ __global__ void __launch_bounds__(kOmpThreads, 1)
       coef_out[(p0 + p) * L + s] = used ? gam[p * L + s] : 0.0f;
     }
     __syncthreads();
+    lap(10);
   }
 }
 
@@ -299,13 +312,13 @@ bool omp_fp32_supported(int n, int K, int L) {
 }
 
 cudaError_t launch_omp_fp32(const float* patches, int64_t N, int n, const float* dict, const double* gram, int K,
-                            int L, int32_t* idx, float* coef, int num_sms, cudaStream_t s) {
+                            int L, int32_t* idx, float* coef, int num_sms, DevStats* stats, cudaStream_t s) {
   size_t smem = omp_fp32_smem_bytes(n, K, L);
   cudaError_t e = cudaFuncSetAttribute(omp_fp32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   int64_t ntiles = (N + kTP - 1) / kTP;
   int grid = int(std::min<int64_t>(ntiles, num_sms));
-  omp_fp32_kernel<<<grid, kOmpThreads, smem, s>>>(patches, N, n, dict, gram, K, L, idx, coef, ntiles);
+  omp_fp32_kernel<<<grid, kOmpThreads, smem, s>>>(patches, N, n, dict, gram, K, L, idx, coef, ntiles, stats);
   return cudaGetLastError();
 }
 

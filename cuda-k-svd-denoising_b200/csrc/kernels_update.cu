@@ -165,159 +165,256 @@ cudaError_t launch_csr_build(const int32_t* idx, const float* coef, int64_t N, i
 
 // ---------------------------------------------------------------------------
 // Persistent update kernel
+//
+// Shared memory: the dictionary (K x n FP32, when it fits; the atoms are
+// updated in place by every CTA, so it never has to be re-read), one chunk of
+// kEChunk residual columns, their metadata (patch, slot, the other atoms and
+// coefficients of the patch), u, the old atom and reduction scratch.
+// The n x n Gram is held in registers in the 16 x 16 thread layout of the
+// phase-A accumulators (TN x TN per thread) and the power iteration runs on
+// it there: v = G u is a per-thread TN x TN block product plus a reduction
+// over the 16 lanes that share a row block.
 // ---------------------------------------------------------------------------
 constexpr int kUpdThreads = 256;
 constexpr int kEChunk = 32;              // residual columns staged per pass
+constexpr int kMinEntriesPerCta = 16;    // phase A uses ceil(c / 16) CTAs at most
 constexpr int kMaxPowerIters = 1000;
 constexpr float kPowerTol = 2.0e-7f;     // max |u_new - u_old| to stop
 
-__host__ __device__ inline size_t update_floats(int n) {
-  size_t a = size_t(kEChunk) * n, b = size_t(n) * (n + 1);
-  return (a > b ? a : b) + 3 * size_t(n) + 64;
+struct UpdLayout {
+  size_t off_ds, off_e, off_mp, off_ms, off_ma, off_mc, off_u, off_dold, off_red, total;
+};
+
+__host__ __device__ inline size_t upd_al16(size_t x) { return (x + 15) & ~size_t(15); }
+
+__host__ __device__ inline UpdLayout upd_layout(int n, int K, int L, bool dsmem) {
+  const int npad = (n + 15) / 16 * 16;
+  UpdLayout o;
+  size_t off = 0;
+  o.off_ds = off;
+  off = upd_al16(off + (dsmem ? size_t(K) * n * 4 : 0));
+  o.off_e = off;
+  off = upd_al16(off + size_t(kEChunk) * n * 4);
+  o.off_mp = off;
+  off = upd_al16(off + kEChunk * 4);
+  o.off_ms = off;
+  off = upd_al16(off + kEChunk * 4);
+  o.off_ma = off;
+  off = upd_al16(off + size_t(kEChunk) * L * 4);
+  o.off_mc = off;
+  off = upd_al16(off + size_t(kEChunk) * L * 4);
+  o.off_u = off;
+  off = upd_al16(off + size_t(npad) * 4);
+  o.off_dold = off;
+  off = upd_al16(off + size_t(npad) * 4);
+  o.off_red = off;
+  off = upd_al16(off + 64 * 4);
+  o.total = off;
+  return o;
 }
 
-// e_p (lane-strided element i) for entry (p, slot): y_p - sum_{s != slot} x_s d_s.
-__device__ __forceinline__ float residual_elem(const float* __restrict__ Y, const float* D, const int32_t* idx,
-                                               const float* coef, int64_t p, int slot, int L, int n, int K, int i) {
-  float e = __ldg(Y + p * n + i);
-  for (int s = 0; s < L; ++s) {
-    if (s == slot) continue;
-    const int a = __ldg(idx + p * L + s);
-    if (a < 0 || a >= K) continue;
-    e = fmaf(-__ldcg(coef + p * L + s), __ldcg(D + int64_t(a) * n + i), e);
-  }
-  return e;
-}
-
-template <int TN>
+template <int TN, bool DSMEM>
 __global__ void __launch_bounds__(kUpdThreads, 1)
     update_kernel(const float* __restrict__ Y, int64_t N, int n, float* D, int K, int L,
                   const int32_t* __restrict__ idx, float* coef, const int* __restrict__ atom_ptr,
                   const int* __restrict__ entries, int q1_cap, float* gpart, float* gsum, GridBarrier* bar,
                   DevStats* stats) {
-  extern __shared__ __align__(16) float sm[];
-  const size_t big = (size_t(kEChunk) * n > size_t(n) * (n + 1)) ? size_t(kEChunk) * n : size_t(n) * (n + 1);
-  float* E = sm;
-  float* Gs = sm;
-  float* u = sm + big;
-  float* dold = u + n;
-  float* spare = dold + n;
-  float* red = spare + n;  // 64 floats
+  extern __shared__ __align__(16) unsigned char usm[];
+  const UpdLayout lo = upd_layout(n, K, L, DSMEM);
+  float* Ds = reinterpret_cast<float*>(usm + lo.off_ds);
+  float* E = reinterpret_cast<float*>(usm + lo.off_e);
+  int* mp = reinterpret_cast<int*>(usm + lo.off_mp);
+  int* ms = reinterpret_cast<int*>(usm + lo.off_ms);
+  int* ma = reinterpret_cast<int*>(usm + lo.off_ma);
+  float* mc = reinterpret_cast<float*>(usm + lo.off_mc);
+  float* u = reinterpret_cast<float*>(usm + lo.off_u);
+  float* dold = reinterpret_cast<float*>(usm + lo.off_dold);
+  float* red = reinterpret_cast<float*>(usm + lo.off_red);
   (void)N;
-  (void)spare;
 
   const unsigned G = gridDim.x;
   const int b = blockIdx.x;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int ti = tid >> 4, tj = tid & 15;
   const int nn = n * n;
+  const int npad = 16 * TN;
+
+  if (DSMEM) {
+    for (int t = tid; t < K * n; t += kUpdThreads) Ds[t] = __ldcg(D + t);
+    __syncthreads();
+  }
+  auto datom = [&](int a, int i) -> float { return DSMEM ? Ds[a * n + i] : __ldcg(D + int64_t(a) * n + i); };
+
+  // Stages metadata of entries [t0, t0 + m) and builds their residual
+  // columns e_p = y_p - sum_{s != slot} x_s d_s into E.
+  auto build_chunk = [&](int beg, int t0, int m) {
+    for (int t = tid; t < kEChunk * L; t += kUpdThreads) {
+      const int q = t / L, s = t - q * L;
+      if (q < m) {
+        const int es = __ldg(entries + beg + t0 + q);
+        const int p = es / L, sl = es - p * L;
+        if (s == 0) {
+          mp[q] = p;
+          ms[q] = sl;
+        }
+        const int a = __ldg(idx + int64_t(p) * L + s);
+        const bool ok = (s != sl) && a >= 0 && a < K;
+        ma[q * L + s] = ok ? a : -1;
+        mc[q * L + s] = ok ? __ldcg(coef + int64_t(p) * L + s) : 0.0f;
+      }
+    }
+    __syncthreads();
+    for (int q = warp; q < kEChunk; q += kUpdThreads / 32) {
+      float* er = E + q * n;
+      if (q < m) {
+        const int64_t p = mp[q];
+        for (int i = lane; i < n; i += 32) {
+          float e = __ldg(Y + p * n + i);
+          for (int s = 0; s < L; ++s) {
+            const int a = ma[q * L + s];
+            if (a >= 0) e = fmaf(-mc[q * L + s], datom(a, i), e);
+          }
+          er[i] = e;
+        }
+      } else {
+        for (int i = lane; i < n; i += 32) er[i] = 0.0f;
+      }
+    }
+    __syncthreads();
+  };
+
+  float blk[TN][TN];
+  const bool timer = (b == 0 && tid == 0);
+  unsigned long long tmark = timer ? globaltimer_ns() : 0ull;
+  auto lap = [&](int slot) {
+    if (timer) {
+      const unsigned long long t = globaltimer_ns();
+      stats->phase_ns[slot] += t - tmark;
+      tmark = t;
+    }
+  };
 
   for (int j = 0; j < K; ++j) {
     const int beg = atom_ptr[j];
     const int c = atom_ptr[j + 1] - beg;
     if (c == 0) continue;
     const int c_eff = (q1_cap && c > 1024) ? 1024 : c;
-    for (int i = tid; i < n; i += kUpdThreads) dold[i] = __ldcg(D + int64_t(j) * n + i);
+    const int active = min(int(G), (c_eff + kMinEntriesPerCta - 1) / kMinEntriesPerCta);
+    for (int i = tid; i < npad; i += kUpdThreads) dold[i] = (i < n) ? datom(j, i) : 0.0f;
 
     // ---- phase A: partial Gram of this CTA's residual columns -------------
-    float acc[TN][TN];
+    const int sb = int(int64_t(c_eff) * b / active), se = int(int64_t(c_eff) * (b + 1) / active);
+    const bool in_a = b < active;
+    if (in_a) {
 #pragma unroll
-    for (int r = 0; r < TN; ++r)
+      for (int r = 0; r < TN; ++r)
 #pragma unroll
-      for (int s = 0; s < TN; ++s) acc[r][s] = 0.0f;
-    const int sb = int(int64_t(c_eff) * b / G), se = int(int64_t(c_eff) * (b + 1) / G);
-    for (int t0 = sb; t0 < se; t0 += kEChunk) {
-      const int m = min(kEChunk, se - t0);
-      for (int q = warp; q < kEChunk; q += kUpdThreads / 32) {
-        float* er = E + q * n;
-        if (q < m) {
-          const int es = __ldg(entries + beg + t0 + q);
-          const int64_t p = es / L;
-          const int slot = es - int(p) * L;
-          for (int i = lane; i < n; i += 32) er[i] = residual_elem(Y, D, idx, coef, p, slot, L, n, K, i);
-        } else {
-          for (int i = lane; i < n; i += 32) er[i] = 0.0f;
+        for (int s = 0; s < TN; ++s) blk[r][s] = 0.0f;
+      for (int t0 = sb; t0 < se; t0 += kEChunk) {
+        const int m = min(kEChunk, se - t0);
+        build_chunk(beg, t0, m);
+        for (int q = 0; q < m; ++q) {
+          const float* er = E + q * n;
+          float ra[TN], rb[TN];
+#pragma unroll
+          for (int r = 0; r < TN; ++r) {
+            const int i = ti + 16 * r;
+            ra[r] = (i < n) ? er[i] : 0.0f;
+          }
+#pragma unroll
+          for (int s = 0; s < TN; ++s) {
+            const int k = tj + 16 * s;
+            rb[s] = (k < n) ? er[k] : 0.0f;
+          }
+#pragma unroll
+          for (int r = 0; r < TN; ++r)
+#pragma unroll
+            for (int s = 0; s < TN; ++s) blk[r][s] = fmaf(ra[r], rb[s], blk[r][s]);
         }
+        if (t0 + kEChunk < se) __syncthreads();  // E is rebuilt by the next chunk
       }
-      __syncthreads();
-      for (int q = 0; q < m; ++q) {
-        const float* er = E + q * n;
-        float ra[TN], rb[TN];
+      float* gp = gpart + size_t(b) * nn;
 #pragma unroll
-        for (int r = 0; r < TN; ++r) {
-          const int i = ti + 16 * r;
-          ra[r] = (i < n) ? er[i] : 0.0f;
-        }
+      for (int r = 0; r < TN; ++r)
 #pragma unroll
         for (int s = 0; s < TN; ++s) {
-          const int k = tj + 16 * s;
-          rb[s] = (k < n) ? er[k] : 0.0f;
+          const int i = ti + 16 * r, k = tj + 16 * s;
+          if (i < n && k < n) gp[i * n + k] = blk[r][s];
         }
-#pragma unroll
-        for (int r = 0; r < TN; ++r)
-#pragma unroll
-          for (int s = 0; s < TN; ++s) acc[r][s] = fmaf(ra[r], rb[s], acc[r][s]);
-      }
-      __syncthreads();
     }
-    float* gp = gpart + size_t(b) * nn;
+    __syncthreads();
+    lap(0);
+    if (!grid_sync(bar, G)) return;
+    lap(1);
+
+    // ---- phase B: fixed-order sum of the active partial Grams --------------
+    {
+      const int qb = int(int64_t(nn) * b / G), qe = int(int64_t(nn) * (b + 1) / G);
+      for (int q = qb + tid; q < qe; q += kUpdThreads) {
+        float s = 0.0f;
+        for (int bb = 0; bb < active; ++bb) s += __ldcg(gpart + size_t(bb) * nn + q);
+        gsum[q] = s;
+      }
+    }
+    __syncthreads();
+    lap(2);
+    if (!grid_sync(bar, G)) return;
+    lap(3);
+
+    // ---- phase C: power iteration on the register-resident Gram ------------
 #pragma unroll
     for (int r = 0; r < TN; ++r)
 #pragma unroll
       for (int s = 0; s < TN; ++s) {
         const int i = ti + 16 * r, k = tj + 16 * s;
-        if (i < n && k < n) gp[i * n + k] = acc[r][s];
+        blk[r][s] = (i < n && k < n) ? __ldcg(gsum + i * n + k) : 0.0f;
       }
-    if (!grid_sync(bar, G)) return;
-
-    // ---- phase B: fixed-order sum of the partial Grams ---------------------
-    {
-      const int qb = int(int64_t(nn) * b / G), qe = int(int64_t(nn) * (b + 1) / G);
-      for (int q = qb + tid; q < qe; q += kUpdThreads) {
-        float s = 0.0f;
-        for (unsigned bb = 0; bb < G; ++bb) s += __ldcg(gpart + size_t(bb) * nn + q);
-        gsum[q] = s;
-      }
-    }
-    if (!grid_sync(bar, G)) return;
-
-    // ---- phase C: top eigenvector by power iteration (same in every CTA) ---
-    for (int q = tid; q < nn; q += kUpdThreads) {
-      const int i = q / n, k = q - i * n;
-      Gs[i * (n + 1) + k] = __ldcg(gsum + q);
-    }
-    for (int i = tid; i < n; i += kUpdThreads) u[i] = dold[i];
+    for (int i = tid; i < npad; i += kUpdThreads) u[i] = dold[i];
     __syncthreads();
     int iters = 0;
     for (int it = 0; it < kMaxPowerIters; ++it) {
-      float vi = 0.0f;
-      if (tid < n) {
-        const float* row = Gs + tid * (n + 1);
-        float s0 = 0.0f, s1 = 0.0f, s2 = 0.0f, s3 = 0.0f;
-        int k = 0;
-        for (; k + 3 < n; k += 4) {
-          s0 = fmaf(row[k], u[k], s0);
-          s1 = fmaf(row[k + 1], u[k + 1], s1);
-          s2 = fmaf(row[k + 2], u[k + 2], s2);
-          s3 = fmaf(row[k + 3], u[k + 3], s3);
-        }
-        for (; k < n; ++k) s0 = fmaf(row[k], u[k], s0);
-        vi = (s0 + s1) + (s2 + s3);
+      float ub[TN], v[TN];
+#pragma unroll
+      for (int s = 0; s < TN; ++s) ub[s] = u[tj + 16 * s];
+#pragma unroll
+      for (int r = 0; r < TN; ++r) {
+        float acc = 0.0f;
+#pragma unroll
+        for (int s = 0; s < TN; ++s) acc = fmaf(blk[r][s], ub[s], acc);
+        v[r] = acc;
       }
-      const float nrm2 = block_sum(vi * vi, red);
+#pragma unroll
+      for (int r = 0; r < TN; ++r) {
+#pragma unroll
+        for (int o = 1; o < 16; o <<= 1) v[r] += __shfl_xor_sync(0xffffffffu, v[r], o);
+      }
+      float part = 0.0f;
+      if (tj == 0) {
+#pragma unroll
+        for (int r = 0; r < TN; ++r) part = fmaf(v[r], v[r], part);
+      }
+      const float nrm2 = block_sum(part, red);
       iters = it + 1;
       if (!(nrm2 > 0.0f)) break;  // E == 0: keep the old atom direction
-      const float vn = vi / sqrtf(nrm2);
-      const float diff = (tid < n) ? fabsf(vn - u[tid]) : 0.0f;
-      const float dmax = block_max(diff, red);
-      if (tid < n) u[tid] = vn;
-      __syncthreads();
+      const float inv = 1.0f / sqrtf(nrm2);
+      float d = 0.0f;
+      if (tj == 0) {
+#pragma unroll
+        for (int r = 0; r < TN; ++r) {
+          const float vn = v[r] * inv;
+          d = fmaxf(d, fabsf(vn - u[ti + 16 * r]));
+          u[ti + 16 * r] = vn;
+        }
+      }
+      const float dmax = block_max(d, red);
       if (dmax < kPowerTol) break;
     }
+    lap(4);
     const float sd = block_sum((tid < n) ? u[tid] * dold[tid] : 0.0f, red);
-    const float sgn = (sd < 0.0f) ? -1.0f : 1.0f;
-    if (tid < n) u[tid] *= sgn;
+    if (sd < 0.0f && tid < n) u[tid] = -u[tid];
     __syncthreads();
+    if (DSMEM)
+      for (int i = tid; i < n; i += kUpdThreads) Ds[j * n + i] = u[i];
     if (b == 0) {
       for (int i = tid; i < n; i += kUpdThreads) D[int64_t(j) * n + i] = u[i];
       if (tid == 0) {
@@ -325,56 +422,78 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
         atomicAdd(&stats->atoms_updated, 1ull);
       }
     }
-    // coefficients of this CTA's slice of all c entries
-    {
-      const int cb = int(int64_t(c) * b / G), ce = int(int64_t(c) * (b + 1) / G);
-      for (int t = cb + warp; t < ce; t += kUpdThreads / 32) {
-        const int es = __ldg(entries + beg + t);
-        if (t >= c_eff) {
-          if (lane == 0) coef[es] = 0.0f;
-          continue;
+
+    // ---- coefficients x_{j,p} = u . e_p ------------------------------------
+    if (in_a) {
+      const bool resident = (se - sb) <= kEChunk;  // E still holds this CTA's columns
+      for (int t0 = sb; t0 < se; t0 += kEChunk) {
+        const int m = min(kEChunk, se - t0);
+        if (!resident) {
+          __syncthreads();
+          build_chunk(beg, t0, m);
         }
-        const int64_t p = es / L;
-        const int slot = es - int(p) * L;
-        float dp = 0.0f;
-        for (int i = lane; i < n; i += 32) dp = fmaf(u[i], residual_elem(Y, D, idx, coef, p, slot, L, n, K, i), dp);
-        dp = warp_sum(dp);
-        if (lane == 0) coef[es] = dp;
+        for (int q = warp; q < m; q += kUpdThreads / 32) {
+          const float* er = E + q * n;
+          float dp = 0.0f;
+          for (int i = lane; i < n; i += 32) dp = fmaf(u[i], er[i], dp);
+          dp = warp_sum(dp);
+          if (lane == 0) coef[int64_t(mp[q]) * L + ms[q]] = dp;
+        }
       }
     }
+    if (c > c_eff) {  // Q1 cap: coefficients beyond the first 1024 entries become 0
+      const int zb = c_eff + int(int64_t(c - c_eff) * b / G), ze = c_eff + int(int64_t(c - c_eff) * (b + 1) / G);
+      for (int t = zb + tid; t < ze; t += kUpdThreads) coef[__ldg(entries + beg + t)] = 0.0f;
+    }
+    __syncthreads();
+    lap(5);
     if (!grid_sync(bar, G)) return;
+    lap(6);
   }
+}
+
+__global__ void accumulate_phases_kernel(const DevStats* __restrict__ src, DevStats* __restrict__ dst) {
+  const int t = threadIdx.x;
+  if (t < 16) dst->phase_ns[t] += src->phase_ns[t];
+}
+
+cudaError_t launch_accumulate_phases(const DevStats* src, DevStats* dst, cudaStream_t s) {
+  accumulate_phases_kernel<<<1, 32, 0, s>>>(src, dst);
+  return cudaGetLastError();
 }
 
 bool update_supported(int n) { return n >= 1 && n <= 160; }
 
-size_t update_smem_bytes(int n) { return update_floats(n) * sizeof(float); }
+static bool dict_in_smem(int n, int K, int L) { return upd_layout(n, K, L, true).total <= 220 * 1024; }
+
+size_t update_smem_bytes(int n, int K, int L) { return upd_layout(n, K, L, dict_in_smem(n, K, L)).total; }
 
 template <int TN>
-static void* update_fn() {
-  return reinterpret_cast<void*>(update_kernel<TN>);
+static void* update_fn(bool dsmem) {
+  return dsmem ? reinterpret_cast<void*>(update_kernel<TN, true>) : reinterpret_cast<void*>(update_kernel<TN, false>);
 }
 
-static void* pick_update(int n) {
+static void* pick_update(int n, bool dsmem) {
   switch ((n + 15) / 16) {
-    case 1: return update_fn<1>();
-    case 2: return update_fn<2>();
-    case 3: return update_fn<3>();
-    case 4: return update_fn<4>();
-    case 5: return update_fn<5>();
-    case 6: return update_fn<6>();
-    case 7: return update_fn<7>();
-    case 8: return update_fn<8>();
-    case 9: return update_fn<9>();
-    case 10: return update_fn<10>();
+    case 1: return update_fn<1>(dsmem);
+    case 2: return update_fn<2>(dsmem);
+    case 3: return update_fn<3>(dsmem);
+    case 4: return update_fn<4>(dsmem);
+    case 5: return update_fn<5>(dsmem);
+    case 6: return update_fn<6>(dsmem);
+    case 7: return update_fn<7>(dsmem);
+    case 8: return update_fn<8>(dsmem);
+    case 9: return update_fn<9>(dsmem);
+    case 10: return update_fn<10>(dsmem);
     default: return nullptr;
   }
 }
 
-int update_grid_size(int n, int num_sms) {
-  void* fn = pick_update(n);
+int update_grid_size(int n, int K, int L, int num_sms) {
+  const bool dsmem = dict_in_smem(n, K, L);
+  void* fn = pick_update(n, dsmem);
   if (!fn) return 0;
-  size_t smem = update_smem_bytes(n);
+  const size_t smem = update_smem_bytes(n, K, L);
   if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess) return 0;
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kUpdThreads, smem) != cudaSuccess) return 0;
@@ -385,18 +504,19 @@ int update_grid_size(int n, int num_sms) {
 cudaError_t launch_update(const float* patches, int64_t N, int n, float* dict, int K, int L, const int32_t* idx,
                           float* coef, CsrWork w, int q1_cap, float* gpart, float* gsum, GridBarrier* bar,
                           DevStats* stats, int grid, cudaStream_t s) {
-  void* fn = pick_update(n);
+  const bool dsmem = dict_in_smem(n, K, L);
+  void* fn = pick_update(n, dsmem);
   if (!fn || grid < 1) return cudaErrorInvalidValue;
-  size_t smem = update_smem_bytes(n);
+  const size_t smem = update_smem_bytes(n, K, L);
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   e = cudaMemsetAsync(bar, 0, sizeof(GridBarrier), s);
   if (e != cudaSuccess) return e;
   const int* atom_ptr = w.atom_ptr;
   const int* entries = w.entries;
-  void* args[] = {(void*)&patches, (void*)&N,       (void*)&n,       (void*)&dict,  (void*)&K,
+  void* args[] = {(void*)&patches, (void*)&N,       (void*)&n,       (void*)&dict,     (void*)&K,
                   (void*)&L,       (void*)&idx,     (void*)&coef,    (void*)&atom_ptr, (void*)&entries,
-                  (void*)&q1_cap,  (void*)&gpart,   (void*)&gsum,    (void*)&bar,   (void*)&stats};
+                  (void*)&q1_cap,  (void*)&gpart,   (void*)&gsum,    (void*)&bar,      (void*)&stats};
   return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kUpdThreads), args, smem, s);
 }
 

@@ -36,6 +36,11 @@ struct DevStats {
   unsigned long long atoms_updated;
   unsigned long long omp_rescore_misses;
   unsigned long long pad;
+  // Wall time (ns) CTA 0 spends in each phase of the persistent kernels:
+  // update: [0] gram build, [1] wait after it, [2] partial sum, [3] wait,
+  // [4] power iteration, [5] coefficients, [6] wait; omp: [8] correlation +
+  // argmax, [9] least squares + residual, [10] tile load/store.
+  unsigned long long phase_ns[16];
 };
 
 // ---------------------------------------------------------------------------
@@ -64,7 +69,8 @@ cudaError_t launch_codes_to_dense(const int32_t* idx, const float* coef, int64_t
 size_t omp_fp32_smem_bytes(int n, int K, int L);
 bool omp_fp32_supported(int n, int K, int L);
 cudaError_t launch_omp_fp32(const float* patches, int64_t N, int n, const float* dict, const double* gram,
-                            int K, int L, int32_t* idx, float* coef, int num_sms, cudaStream_t s);
+                            int K, int L, int32_t* idx, float* coef, int num_sms, DevStats* stats,
+                            cudaStream_t s);
 
 // Dictionary update.
 struct CsrWork {
@@ -77,8 +83,9 @@ int64_t csr_num_chunks(int64_t N);
 cudaError_t launch_csr_build(const int32_t* idx, const float* coef, int64_t N, int L, int K, CsrWork w,
                              cudaStream_t s);
 bool update_supported(int n);
-size_t update_smem_bytes(int n);
-int update_grid_size(int n, int num_sms);
+cudaError_t launch_accumulate_phases(const DevStats* src, DevStats* dst, cudaStream_t s);
+size_t update_smem_bytes(int n, int K, int L);
+int update_grid_size(int n, int K, int L, int num_sms);
 cudaError_t launch_update(const float* patches, int64_t N, int n, float* dict, int K, int L,
                           const int32_t* idx, float* coef, CsrWork w, int q1_cap, float* gpart,
                           float* gsum, GridBarrier* bar, DevStats* stats, int grid, cudaStream_t s);
@@ -124,5 +131,6 @@ struct ksvd_ctx {
   int64_t launch_count = 0;
 
   ksvd::GridBarrier* d_flags = nullptr;  // error flag word + barrier
-  ksvd::DevStats* d_stats = nullptr;
+  ksvd::DevStats* d_stats = nullptr;      // per-call counters
+  ksvd::DevStats* d_phase = nullptr;      // phase timers, accumulated while profiling
 };

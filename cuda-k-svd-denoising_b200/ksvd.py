@@ -140,6 +140,8 @@ def lib():
         L.ksvd_profile_reset.restype = _int
         L.ksvd_launch_count.argtypes = [_vp]
         L.ksvd_launch_count.restype = _i64
+        L.ksvd_profile_phases.argtypes = [_vp, ctypes.POINTER(ctypes.c_double), _int]
+        L.ksvd_profile_phases.restype = _int
         _lib = L
     return _lib
 
@@ -286,6 +288,11 @@ class Context:
         n = _i64(0)
         self._check(lib().ksvd_profile_read(self.h, family.encode(), ctypes.byref(ms), ctypes.byref(n)))
         return ms.value, n.value
+
+    def profile_phases(self) -> list:
+        arr = (ctypes.c_double * 16)()
+        self._check(lib().ksvd_profile_phases(self.h, arr, 16))
+        return list(arr)
 
     def launch_count(self) -> int:
         return int(lib().ksvd_launch_count(self.h))

@@ -201,6 +201,12 @@ ksvd_status ksvd_profile_read(ksvd_ctx* ctx, const char* family, double* total_m
 ksvd_status ksvd_profile_reset(ksvd_ctx* ctx);
 /* Total number of kernels this context launched since creation. */
 int64_t ksvd_launch_count(const ksvd_ctx* ctx);
+/* Wall time (ms) the first CTA of the persistent kernels spent per phase
+ * while profiling was enabled (since the last reset): [0] update Gram build,
+ * [1] grid wait, [2] partial-Gram sum, [3] grid wait, [4] power iteration,
+ * [5] coefficients, [6] grid wait, [8] OMP correlation + argmax, [9] OMP least
+ * squares + residual, [10] OMP tile load/store.  Synchronises the stream. */
+ksvd_status ksvd_profile_phases(ksvd_ctx* ctx, double* ms_out, int count);
 
 #ifdef __cplusplus
 }
