@@ -355,7 +355,8 @@ def main():
             "phase_ms_per_step": {
                 name: phases[i] / max(args.steps, 1) for i, name in (
                     (0, "upd_gram"), (1, "upd_wait1"), (2, "upd_sum"), (3, "upd_wait2"), (4, "upd_power"),
-                    (5, "upd_coef"), (6, "upd_wait3"), (8, "omp_corr"), (9, "omp_ls"), (10, "omp_io"))},
+                    (5, "upd_coef"), (6, "upd_wait3"), (8, "omp_corr"), (9, "omp_ls"), (10, "omp_io"),
+                    (11, "upd_gram_stage"), (12, "upd_gram_finish"), (13, "upd_gram_acc"), (14, "upd_gload"))},
             "quality": {"psnr_noisy": psnr_noisy, "psnr_denoised": psnr_out,
                         "power_iters_last_sweep": st.power_iters, "atoms_updated_last_sweep": st.atoms_updated},
             "clocks": clocks.summary(),

@@ -149,11 +149,14 @@ ksvd_status validate_params(const ksvd_params* p, std::string* why) {
 
 ksvd_status check_kernel_support(ksvd_ctx* c) {
   const int n = c->p.patch_width_dim * c->p.patch_height_dim;
-  if (!ksvd::omp_fp32_supported(n, c->p.atoms, c->p.omp_iter))
-    return fail(c, KSVD_ERR_INVALID, "patch size x atoms too large for the resident-dictionary OMP kernel");
+  if (c->p.precision == KSVD_PREC_FP32) {
+    if (!ksvd::omp_fp32_supported(n, c->p.atoms, c->p.omp_iter))
+      return fail(c, KSVD_ERR_INVALID, "patch size x atoms too large for the resident-dictionary OMP kernel");
+  } else {
+    if (!ksvd::omp_tc_supported(n, c->p.atoms, c->p.omp_iter))
+      return fail(c, KSVD_ERR_INVALID, "patch size x atoms too large for the tensor-core OMP kernel");
+  }
   if (!ksvd::update_supported(n)) return fail(c, KSVD_ERR_INVALID, "patch size > 160 not supported by the update kernel");
-  if (c->p.precision != KSVD_PREC_FP32)
-    return fail(c, KSVD_ERR_INVALID, "BF16 correlation path not available in this build");
   return KSVD_OK;
 }
 
@@ -384,10 +387,17 @@ static ksvd_status omp_impl(ksvd_ctx* c, const float* d_patches, int64_t N, cons
     KSVD_CU(c, ksvd::launch_gram_f64(d_dict, K, n, gram, c->stream), "gram");
   }
   Prof pr(c, "omp", 1);
-  KSVD_CU(c,
-          ksvd::launch_omp_fp32(d_patches, N, n, d_dict, gram, K, L, d_idx, d_coef, c->num_sms,
+  if (c->p.precision == KSVD_PREC_BF16_RESCORE) {
+    KSVD_CU(c,
+            ksvd::launch_omp_tc(d_patches, N, n, d_dict, gram, K, L, d_idx, d_coef, c->num_sms, c->d_flags,
                                 c->profiling ? c->d_phase : nullptr, c->stream),
-          "omp");
+            "omp (tensor cores)");
+  } else {
+    KSVD_CU(c,
+            ksvd::launch_omp_fp32(d_patches, N, n, d_dict, gram, K, L, d_idx, d_coef, c->num_sms,
+                                  c->profiling ? c->d_phase : nullptr, c->stream),
+            "omp");
+  }
   return KSVD_OK;
 }
 
@@ -396,7 +406,9 @@ ksvd_status ksvd_omp(ksvd_ctx* c, const float* d_patches, int64_t N, const float
   KSVD_TRY(check_ctx(c));
   if (!d_patches || !d_dict || !d_idx || !d_coef || N < 1) return fail(c, KSVD_ERR_INVALID, "bad argument");
   KSVD_TRY(check_kernel_support(c));
-  return omp_impl(c, d_patches, N, d_dict, d_idx, d_coef);
+  KSVD_TRY(omp_impl(c, d_patches, N, d_dict, d_idx, d_coef));
+  if (c->p.precision == KSVD_PREC_BF16_RESCORE) return check_dev_flags(c, "omp");
+  return KSVD_OK;
 }
 
 static ksvd_status update_impl(ksvd_ctx* c, const float* d_patches, int64_t N, float* d_dict, const int32_t* d_idx,
@@ -407,11 +419,14 @@ static ksvd_status update_impl(ksvd_ctx* c, const float* d_patches, int64_t N, f
   KSVD_TRY(wsT(c, "csr_counts", size_t(w.nchunks) * K, &w.chunk_counts));
   KSVD_TRY(wsT(c, "csr_atom_ptr", size_t(2) * K + 1, &w.atom_ptr));
   KSVD_TRY(wsT(c, "csr_entries", size_t(N) * L, &w.entries));
+  KSVD_TRY(wsT(c, "csr_records", size_t(N) * L * ksvd::csr_record_ints(L), &w.records));
   const int grid = ksvd::update_grid_size(n, K, L, c->num_sms);
   if (grid < 1) return fail(c, KSVD_ERR_CUDA, "update kernel cannot be made co-resident");
-  float *gpart = nullptr, *gsum = nullptr;
+  float *gpart = nullptr, *gsum = nullptr, *escr = nullptr;
   KSVD_TRY(wsT(c, "upd_gpart", size_t(grid) * n * n, &gpart));
   KSVD_TRY(wsT(c, "upd_gsum", size_t(n) * n, &gsum));
+  const int64_t escr_cap = ksvd::update_scratch_cap(N, grid);
+  KSVD_TRY(wsT(c, "upd_escr", size_t(grid) * size_t(escr_cap) * n, &escr));
   {
     Prof pr(c, "csr", 4);
     KSVD_CU(c, ksvd::launch_csr_build(d_idx, d_coef, N, L, K, w, c->stream), "csr build");
@@ -420,8 +435,8 @@ static ksvd_status update_impl(ksvd_ctx* c, const float* d_patches, int64_t N, f
   Prof pr(c, "update", 1);
   KSVD_CU(c,
           ksvd::launch_update(d_patches, N, n, d_dict, K, L, d_idx, d_coef, w,
-                              (c->p.compat & KSVD_COMPAT_Q1_CAP) ? 1 : 0, gpart, gsum, c->d_flags, c->d_stats,
-                              grid, c->stream),
+                              (c->p.compat & KSVD_COMPAT_Q1_CAP) ? 1 : 0, gpart, gsum, escr, escr_cap, c->d_flags,
+                              c->d_stats, grid, c->stream),
           "update");
   if (c->profiling) {
     // fold this sweep's phase timers into the profiling accumulator

@@ -68,6 +68,32 @@ __device__ T block_sum(T v, T* red) {
   return red[0];
 }
 
+// Block-wide sum of a pair; `red` holds at least 64 floats.
+__device__ inline float2 block_sum2(float2 v, float* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = (blockDim.x + 31) >> 5;
+  v.x = warp_sum(v.x);
+  v.y = warp_sum(v.y);
+  __syncthreads();
+  if (lane == 0) {
+    red[2 * warp] = v.x;
+    red[2 * warp + 1] = v.y;
+  }
+  __syncthreads();
+  float2 t = (threadIdx.x < nw) ? make_float2(red[2 * threadIdx.x], red[2 * threadIdx.x + 1]) : make_float2(0.f, 0.f);
+  if (warp == 0) {
+    t.x = warp_sum(t.x);
+    t.y = warp_sum(t.y);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    red[0] = t.x;
+    red[1] = t.y;
+  }
+  __syncthreads();
+  return make_float2(red[0], red[1]);
+}
+
 __device__ inline float block_max(float v, float* red) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nw = (blockDim.x + 31) >> 5;
@@ -117,6 +143,53 @@ __device__ inline bool grid_sync(GridBarrier* b, unsigned nblocks) {
   }
   __syncthreads();
   return s_ok != 0;
+}
+
+// ---------------------------------------------------------------------------
+// mbarrier + bulk (TMA) copies global -> shared.
+// ---------------------------------------------------------------------------
+KSVD_DEV unsigned smem_u32(const void* p) { return static_cast<unsigned>(__cvta_generic_to_shared(p)); }
+
+KSVD_DEV void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+KSVD_DEV void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+// Orders this thread's generic-proxy shared-memory accesses before later
+// async-proxy (bulk copy) accesses of the same bytes.
+KSVD_DEV void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+KSVD_DEV void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+// 1-D bulk copy; dst, src 16-byte aligned, bytes a multiple of 16.
+KSVD_DEV void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+KSVD_DEV bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Waits for the phase with the given parity to complete, at most timeout_ns.
+KSVD_DEV bool mbar_wait(unsigned long long* bar, unsigned parity, unsigned long long timeout_ns) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = globaltimer_ns();
+  while (!mbar_try_wait(bar, parity))
+    if (globaltimer_ns() - t0 > timeout_ns) return false;
+  return true;
 }
 
 }  // namespace ksvd

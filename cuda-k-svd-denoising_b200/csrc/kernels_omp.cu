@@ -30,9 +30,9 @@ constexpr int kAtomBlock = 256;  // atoms per register-tiled pass (32 groups x 8
 constexpr int kLMax = 32;        // omp_iter limit (support list fits a warp)
 
 struct OmpLayout {
-  int Kpad, dks, rks;
+  int Kpad, dks, rks, ysn;
   size_t off_dk, off_rk, off_ys, off_lc, off_bv, off_s, off_gam, off_sel, off_cnt, off_done, off_redv, off_redi,
-      total;
+      off_gs, off_bs, off_np, total;
 };
 
 __host__ __device__ inline size_t al16(size_t x) { return (x + 15) & ~size_t(15); }
@@ -42,13 +42,14 @@ __host__ __device__ inline OmpLayout omp_layout(int n, int K, int L) {
   o.Kpad = (K + kAtomBlock - 1) / kAtomBlock * kAtomBlock;
   o.dks = o.Kpad + 4;
   o.rks = kTP + 4;
+  o.ysn = n + 1;  // odd row stride: lanes over patches hit distinct banks
   size_t off = 0;
   o.off_dk = off;
   off = al16(off + size_t(n) * o.dks * 4);
   o.off_rk = off;
   off = al16(off + size_t(n) * o.rks * 4);
   o.off_ys = off;
-  off = al16(off + size_t(kTP) * n * 4);
+  off = al16(off + size_t(kTP) * o.ysn * 4);
   o.off_lc = off;
   off = al16(off + size_t(kTP) * L * L * 8);
   o.off_bv = off;
@@ -66,6 +67,12 @@ __host__ __device__ inline OmpLayout omp_layout(int n, int K, int L) {
   o.off_redv = off;
   off = al16(off + 8 * kTP * 4);
   o.off_redi = off;
+  off = al16(off + 8 * kTP * 4);
+  o.off_gs = off;
+  off = al16(off + size_t(kTP) * (L + 1) * 8);
+  o.off_bs = off;
+  off = al16(off + kTP * 8);
+  o.off_np = off;
   off = al16(off + 8 * kTP * 4);
   o.total = off;
   return o;
@@ -93,6 +100,10 @@ __global__ void __launch_bounds__(kOmpThreads, 1)
   int* done = reinterpret_cast<int*>(smem + lo.off_done);
   float* redv = reinterpret_cast<float*>(smem + lo.off_redv);
   int* redi = reinterpret_cast<int*>(smem + lo.off_redi);
+  double* gS = reinterpret_cast<double*>(smem + lo.off_gs);
+  double* bS = reinterpret_cast<double*>(smem + lo.off_bs);
+  float* npart = reinterpret_cast<float*>(smem + lo.off_np);
+  const int ysn = lo.ysn;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int dks = lo.dks, rks = lo.rks, Kpad = lo.Kpad;
@@ -129,7 +140,7 @@ __global__ void __launch_bounds__(kOmpThreads, 1)
     for (int t = tid; t < kTP * n; t += kOmpThreads) {
       int p = t / n, k = t - p * n;
       float v = (p < np) ? __ldg(Yt + t) : 0.0f;
-      Ys[t] = v;
+      Ys[p * ysn + k] = v;
       Rk[k * rks + p] = v;
     }
     if (tid < kTP) {
@@ -222,72 +233,92 @@ __global__ void __launch_bounds__(kOmpThreads, 1)
       lap(8);
 
       // ---- least squares on the grown support, residual, norm -------------
-      for (int q = 0; q < kTP / 8; ++q) {
-        const int p = warp + 8 * q;
+      // (1) dependence test and support-Gram column, all patches at once:
+      //     gS[p][i] = G[S_i][a] (i < k), gS[p][k] = G[a][a]
+      for (int t = tid; t < kTP * (L + 1); t += kOmpThreads) {
+        const int p = t / (L + 1), i = t - p * (L + 1);
         if (done[p]) continue;
-        const int a = sel[p];
-        const int k = cnt[p];
-        const bool dup = (lane < k) && (S[p * L + lane] == a);
-        if (__any_sync(0xffffffffu, dup)) {
-          if (lane == 0) done[p] = 1;
-          continue;
+        const int k = cnt[p], a = sel[p];
+        if (i < k) {
+          const int si = S[p * L + i];
+          if (si == a) done[p] = 2;  // re-selected atom: the pursuit of p ends
+          gS[p * (L + 1) + i] = Gram[int64_t(si) * K + a];
+        } else if (i == k) {
+          gS[p * (L + 1) + i] = Gram[int64_t(a) * K + a];
         }
-        // b = d_a . y in FP64
+      }
+      // (2) b_p = d_a . y_p in FP64, four patches per warp
+      for (int q = 0; q < kTP / 8; ++q) {
+        const int p = warp * (kTP / 8) + q;
+        const int a = sel[p];
         double bp = 0.0;
-        const float* da = D + int64_t(a) * n;
-        const float* yp = Ys + p * n;
-        for (int i = lane; i < n; i += 32) bp = fma(double(__ldg(da + i)), double(yp[i]), bp);
+        for (int k = lane; k < n; k += 32) bp = fma(double(Dk[k * dks + a]), double(Ys[p * ysn + k]), bp);
         bp = warp_sum(bp);
-        int ok = 1;
-        if (lane == 0) {
+        if (lane == 0) bS[p] = bp;
+      }
+      __syncthreads();
+      // (3) Cholesky row append and solve, one thread per patch
+      if (tid < kTP) {
+        const int p = tid;
+        if (done[p] == 2) done[p] = 1;
+        if (!done[p]) {
+          const int k = cnt[p], a = sel[p];
           double* Lp = Lc + p * L * L;
+          const double* g = gS + p * (L + 1);
           double ww = 0.0;
           for (int i = 0; i < k; ++i) {
-            double s = Gram[int64_t(S[p * L + i]) * K + a];
-            for (int j = 0; j < i; ++j) s -= Lp[i * L + j] * Lp[k * L + j];
-            double wi = s / Lp[i * L + i];
+            double s = g[i];
+            for (int j2 = 0; j2 < i; ++j2) s -= Lp[i * L + j2] * Lp[k * L + j2];
+            const double wi = s / Lp[i * L + i];
             Lp[k * L + i] = wi;
             ww += wi * wi;
           }
-          double piv2 = Gram[int64_t(a) * K + a] - ww;
+          const double piv2 = g[k] - ww;
           if (!(piv2 > 0.0)) {
-            ok = 0;
+            done[p] = 1;  // the new atom depends linearly on the support
           } else {
             Lp[k * L + k] = sqrt(piv2);
             S[p * L + k] = a;
-            bvec[p * L + k] = bp;
+            bvec[p * L + k] = bS[p];
             cnt[p] = k + 1;
-            // solve L L^T g = b
             double yv[kLMax];
             for (int i = 0; i <= k; ++i) {
               double s = bvec[p * L + i];
-              for (int j = 0; j < i; ++j) s -= Lp[i * L + j] * yv[j];
+              for (int j2 = 0; j2 < i; ++j2) s -= Lp[i * L + j2] * yv[j2];
               yv[i] = s / Lp[i * L + i];
             }
             for (int i = k; i >= 0; --i) {
               double s = yv[i];
-              for (int j = i + 1; j <= k; ++j) s -= Lp[j * L + i] * yv[j];
+              for (int j2 = i + 1; j2 <= k; ++j2) s -= Lp[j2 * L + i] * yv[j2];
               yv[i] = s / Lp[i * L + i];
             }
             for (int i = 0; i <= k; ++i) gam[p * L + i] = float(yv[i]);
           }
         }
-        ok = __shfl_sync(0xffffffffu, ok, 0);
-        if (!ok) {
-          if (lane == 0) done[p] = 1;
-          continue;
-        }
-        __syncwarp();
-        const int kk = k + 1;
+      }
+      __syncthreads();
+      // (4) residual r = y - D_S g (lanes over patches, warps over row chunks)
+      {
+        const int p = lane;
+        const int rows = (n + 7) / 8;
+        const int k0 = warp * rows, k1 = min(n, k0 + rows);
         float nrm = 0.0f;
-        for (int i = lane; i < n; i += 32) {
-          float r = yp[i];
-          for (int s = 0; s < kk; ++s) r = fmaf(-gam[p * L + s], __ldg(D + int64_t(S[p * L + s]) * n + i), r);
-          Rk[i * rks + p] = r;
-          nrm = fmaf(r, r, nrm);
+        if (!done[p]) {
+          const int kk = cnt[p];
+          for (int k = k0; k < k1; ++k) {
+            float r = Ys[p * ysn + k];
+            for (int s2 = 0; s2 < kk; ++s2) r = fmaf(-gam[p * L + s2], Dk[k * dks + S[p * L + s2]], r);
+            Rk[k * rks + p] = r;
+            nrm = fmaf(r, r, nrm);
+          }
         }
-        nrm = warp_sum(nrm);
-        if (lane == 0 && sqrtf(nrm) < 1e-3f) done[p] = 1;
+        npart[warp * kTP + p] = nrm;
+      }
+      __syncthreads();
+      if (tid < kTP && !done[tid]) {
+        float nrm = 0.0f;
+        for (int w = 0; w < 8; ++w) nrm += npart[w * kTP + tid];
+        if (sqrtf(nrm) < 1e-3f) done[tid] = 1;
       }
       __syncthreads();
       lap(9);

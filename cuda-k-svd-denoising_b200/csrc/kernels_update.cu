@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(kCsrChunk) csr_fill_kernel(const int32_t* __re
                                                              const float* __restrict__ coef, int64_t N, int L,
                                                              int K, int64_t nchunks, const int* __restrict__ counts,
                                                              const int* __restrict__ atom_ptr,
-                                                             int* __restrict__ entries) {
+                                                             int* __restrict__ entries, int* __restrict__ records) {
   extern __shared__ int csr_sm[];
   int* wcnt = csr_sm;              // 8 x K
   int* watoms = csr_sm + 8 * K;    // 8 x 32 x L
@@ -137,7 +137,14 @@ __global__ void __launch_bounds__(kCsrChunk) csr_fill_kernel(const int32_t* __re
     int rank = 0;
     for (int l2 = 0; l2 < lane; ++l2)
       for (int s2 = 0; s2 < L; ++s2) rank += (wa[l2 * L + s2] == a);
-    entries[wcnt[warp * K + a] + rank] = int(p * L + s);
+    const int pos = wcnt[warp * K + a] + rank;
+    entries[pos] = int(p * L + s);
+    const int R = (L + 2 + 3) / 4 * 4;
+    int* rec = records + int64_t(pos) * R;
+    rec[0] = int(p);
+    rec[1] = s;
+    for (int s2 = 0; s2 < L; ++s2) rec[2 + s2] = mine[s2];
+    for (int r2 = L + 2; r2 < R; ++r2) rec[r2] = -1;
   }
 }
 
@@ -159,7 +166,7 @@ cudaError_t launch_csr_build(const int32_t* idx, const float* coef, int64_t N, i
     if (e != cudaSuccess) return e;
   }
   csr_fill_kernel<<<unsigned(nch), kCsrChunk, smem, s>>>(idx, coef, N, L, K, nch, w.chunk_counts, w.atom_ptr,
-                                                         w.entries);
+                                                         w.entries, w.records);
   return cudaGetLastError();
 }
 
@@ -176,60 +183,71 @@ cudaError_t launch_csr_build(const int32_t* idx, const float* coef, int64_t N, i
 // over the 16 lanes that share a row block.
 // ---------------------------------------------------------------------------
 constexpr int kUpdThreads = 256;
-constexpr int kEChunk = 32;              // residual columns staged per pass
+constexpr int kEChunk = 32;              // residual columns per pipeline stage
 constexpr int kMinEntriesPerCta = 16;    // phase A uses ceil(c / 16) CTAs at most
 constexpr int kMaxPowerIters = 1000;
 constexpr float kPowerTol = 2.0e-7f;     // max |u_new - u_old| to stop
+constexpr unsigned long long kCopyWaitNs = 2000000000ull;  // bound of one bulk-copy wait
 
 struct UpdLayout {
-  size_t off_ds, off_e, off_mp, off_ms, off_ma, off_mc, off_u, off_dold, off_red, total;
+  size_t off_ds, off_e, off_rec, off_cf, off_u, off_dold, off_red, off_bar, total;
 };
 
 __host__ __device__ inline size_t upd_al16(size_t x) { return (x + 15) & ~size_t(15); }
 
+// Two residual-column buffers, three record buffers, two gathered-coefficient
+// buffers, the mbarriers (3 for records, 2 for columns).
 __host__ __device__ inline UpdLayout upd_layout(int n, int K, int L, bool dsmem) {
   const int npad = (n + 15) / 16 * 16;
+  const int R = (L + 2 + 3) / 4 * 4;
   UpdLayout o;
   size_t off = 0;
   o.off_ds = off;
   off = upd_al16(off + (dsmem ? size_t(K) * n * 4 : 0));
   o.off_e = off;
-  off = upd_al16(off + size_t(kEChunk) * n * 4);
-  o.off_mp = off;
-  off = upd_al16(off + kEChunk * 4);
-  o.off_ms = off;
-  off = upd_al16(off + kEChunk * 4);
-  o.off_ma = off;
-  off = upd_al16(off + size_t(kEChunk) * L * 4);
-  o.off_mc = off;
-  off = upd_al16(off + size_t(kEChunk) * L * 4);
+  off = upd_al16(off + size_t(2) * kEChunk * n * 4);
+  o.off_rec = off;
+  off = upd_al16(off + size_t(3) * kEChunk * R * 4);
+  o.off_cf = off;
+  off = upd_al16(off + size_t(2) * kEChunk * L * 4);
   o.off_u = off;
   off = upd_al16(off + size_t(npad) * 4);
   o.off_dold = off;
   off = upd_al16(off + size_t(npad) * 4);
   o.off_red = off;
   off = upd_al16(off + 64 * 4);
+  o.off_bar = off;
+  off = upd_al16(off + 5 * 8);
   o.total = off;
   return o;
 }
+
+KSVD_DEV void bulk_s2g(void* gdst, const void* ssrc, unsigned bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gdst), "r"(smem_u32(ssrc)),
+               "r"(bytes)
+               : "memory");
+}
+KSVD_DEV void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+KSVD_DEV void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+KSVD_DEV void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
 template <int TN, bool DSMEM>
 __global__ void __launch_bounds__(kUpdThreads, 1)
     update_kernel(const float* __restrict__ Y, int64_t N, int n, float* D, int K, int L,
                   const int32_t* __restrict__ idx, float* coef, const int* __restrict__ atom_ptr,
-                  const int* __restrict__ entries, int q1_cap, float* gpart, float* gsum, GridBarrier* bar,
-                  DevStats* stats) {
+                  const int* __restrict__ entries, const int* __restrict__ records, int q1_cap, int tma,
+                  float* gpart, float* gsum, float* escr, int64_t escr_cap, GridBarrier* bar, DevStats* stats) {
   extern __shared__ __align__(16) unsigned char usm[];
   const UpdLayout lo = upd_layout(n, K, L, DSMEM);
+  const int R = (L + 2 + 3) / 4 * 4;
   float* Ds = reinterpret_cast<float*>(usm + lo.off_ds);
-  float* E = reinterpret_cast<float*>(usm + lo.off_e);
-  int* mp = reinterpret_cast<int*>(usm + lo.off_mp);
-  int* ms = reinterpret_cast<int*>(usm + lo.off_ms);
-  int* ma = reinterpret_cast<int*>(usm + lo.off_ma);
-  float* mc = reinterpret_cast<float*>(usm + lo.off_mc);
+  float* Ebase = reinterpret_cast<float*>(usm + lo.off_e);
+  int* recb = reinterpret_cast<int*>(usm + lo.off_rec);
+  float* cfb = reinterpret_cast<float*>(usm + lo.off_cf);
   float* u = reinterpret_cast<float*>(usm + lo.off_u);
   float* dold = reinterpret_cast<float*>(usm + lo.off_dold);
   float* red = reinterpret_cast<float*>(usm + lo.off_red);
+  unsigned long long* bars = reinterpret_cast<unsigned long long*>(usm + lo.off_bar);  // [0..2] rec, [3..4] col
   (void)N;
 
   const unsigned G = gridDim.x;
@@ -238,49 +256,122 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
   const int ti = tid >> 4, tj = tid & 15;
   const int nn = n * n;
   const int npad = 16 * TN;
+  float* my_escr = escr + size_t(b) * size_t(escr_cap) * n;
 
-  if (DSMEM) {
-    for (int t = tid; t < K * n; t += kUpdThreads) Ds[t] = __ldcg(D + t);
-    __syncthreads();
+  if (tid == 0) {
+    for (int k = 0; k < 5; ++k) mbar_init(&bars[k], 1);
+    fence_mbar_init();
   }
-  auto datom = [&](int a, int i) -> float { return DSMEM ? Ds[a * n + i] : __ldcg(D + int64_t(a) * n + i); };
+  if (DSMEM)
+    for (int t = tid; t < K * n; t += kUpdThreads) Ds[t] = __ldcg(D + t);
+  __syncthreads();
+  // parity bit of the next phase of each mbarrier; only thread 0 waits on
+  // record barriers, every thread waits on column barriers.
+  unsigned parity = 0;
+  bool failed = false;  // thread 0: a bulk-copy wait timed out
 
-  // Stages metadata of entries [t0, t0 + m) and builds their residual
-  // columns e_p = y_p - sum_{s != slot} x_s d_s into E.
-  auto build_chunk = [&](int beg, int t0, int m) {
-    for (int t = tid; t < kEChunk * L; t += kUpdThreads) {
-      const int q = t / L, s = t - q * L;
-      if (q < m) {
-        const int es = __ldg(entries + beg + t0 + q);
-        const int p = es / L, sl = es - p * L;
-        if (s == 0) {
-          mp[q] = p;
-          ms[q] = sl;
-        }
-        const int a = __ldg(idx + int64_t(p) * L + s);
-        const bool ok = (s != sl) && a >= 0 && a < K;
-        ma[q * L + s] = ok ? a : -1;
-        mc[q * L + s] = ok ? __ldcg(coef + int64_t(p) * L + s) : 0.0f;
+  auto datom = [&](int a, int i) -> float { return DSMEM ? Ds[a * n + i] : __ldcg(D + int64_t(a) * n + i); };
+  auto wait_bar = [&](int k) -> bool {
+    const bool ok = mbar_wait(&bars[k], (parity >> k) & 1u, kCopyWaitNs);
+    parity ^= (1u << k);
+    return ok;
+  };
+
+  // ---- pipeline stages (thread 0 issues every bulk copy) -------------------
+  // records of chunk [t0, t0+m) of atom entries starting at beg -> ring slot r3
+  auto issue_records = [&](int beg, int t0, int m, int r3) {
+    if (tid == 0 && !failed) {
+      mbar_arrive_expect_tx(&bars[r3], unsigned(m * R * 4));
+      bulk_g2s(recb + r3 * kEChunk * R, records + int64_t(beg + t0) * R, unsigned(m * R * 4), &bars[r3]);
+    }
+  };
+  // patches of the chunk whose records sit in ring slot r3 -> column buffer buf
+  auto issue_patches = [&](int m, int r3, int buf, bool rec_waited) {
+    if (tid == 0 && !failed) {
+      if (!rec_waited && !wait_bar(r3)) {
+        failed = true;
+        return;
+      }
+      const int* rc = recb + r3 * kEChunk * R;
+      float* Eb = Ebase + size_t(buf) * kEChunk * n;
+      bulk_wait_read0();  // scratch stores out of this buffer have read it
+      if (tma) {
+        mbar_arrive_expect_tx(&bars[3 + buf], unsigned(m) * unsigned(n) * 4u);
+        for (int q = 0; q < m; ++q) bulk_g2s(Eb + q * n, Y + int64_t(rc[q * R]) * n, unsigned(n) * 4u, &bars[3 + buf]);
       }
     }
-    __syncthreads();
-    for (int q = warp; q < kEChunk; q += kUpdThreads / 32) {
-      float* er = E + q * n;
-      if (q < m) {
-        const int64_t p = mp[q];
-        for (int i = lane; i < n; i += 32) {
-          float e = __ldg(Y + p * n + i);
-          for (int s = 0; s < L; ++s) {
-            const int a = ma[q * L + s];
-            if (a >= 0) e = fmaf(-mc[q * L + s], datom(a, i), e);
-          }
-          er[i] = e;
+  };
+  // Other-slot coefficients of the chunk whose records sit in ring slot r3:
+  // each thread loads up to kCfRegs of them into registers (prefetch) and
+  // later stores them into cf buffer `buf`.
+  constexpr int kCfRegs = 4;
+  auto gather_load = [&](int m, int r3, float (&vals)[kCfRegs]) {
+    const int* rc = recb + r3 * kEChunk * R;
+#pragma unroll
+    for (int g = 0; g < kCfRegs; ++g) {
+      const int t = tid + g * kUpdThreads;
+      float v = 0.0f;
+      if (t < m * L) {
+        const int q = t / L, s2 = t - q * L;
+        const int a = rc[q * R + 2 + s2];
+        if (s2 != rc[q * R + 1] && a >= 0) v = __ldcg(coef + int64_t(rc[q * R]) * L + s2);
+      }
+      vals[g] = v;
+    }
+  };
+  auto gather_store = [&](int m, int buf, const float (&vals)[kCfRegs]) {
+    float* cf = cfb + buf * kEChunk * L;
+#pragma unroll
+    for (int g = 0; g < kCfRegs; ++g) {
+      const int t = tid + g * kUpdThreads;
+      if (t < m * L) cf[t] = vals[g];
+    }
+  };
+  // Waits for the columns of buffer buf (records in r3, coefficients already
+  // in cf buffer buf), subtracts the other atoms in place and (store=true)
+  // copies the finished columns to this CTA's scratch at column offset soff.
+  auto finish = [&](int m, int r3, int buf, bool store, int soff) -> bool {
+    const int* rc = recb + r3 * kEChunk * R;
+    float* Eb = Ebase + size_t(buf) * kEChunk * n;
+    const float* cf = cfb + buf * kEChunk * L;
+    bool ok = true;
+    if (tma) ok = wait_bar(3 + buf);
+    if (__syncthreads_or(!ok || (tid == 0 && failed))) {
+      if (tid == 0) atomicCAS(&bar->err, DEVERR_NONE, DEVERR_TIMEOUT);
+      return false;
+    }
+    if (!tma) {  // generic loads when rows are not 16-byte aligned
+      for (int q = warp; q < m; q += kUpdThreads / 32)
+        for (int i = lane; i < n; i += 32) Eb[q * n + i] = __ldg(Y + int64_t(rc[q * R]) * n + i);
+      __syncthreads();
+    }
+    for (int q = warp; q < m; q += kUpdThreads / 32) {
+      const int* rq = rc + q * R;
+      for (int i = lane; i < n; i += 32) {
+        float e = Eb[q * n + i];
+        for (int s2 = 0; s2 < L; ++s2) {
+          const float cv = cf[q * L + s2];
+          if (cv != 0.0f) e = fmaf(-cv, datom(rq[2 + s2], i), e);
         }
-      } else {
-        for (int i = lane; i < n; i += 32) er[i] = 0.0f;
+        Eb[q * n + i] = e;
       }
     }
+    fence_proxy_async_smem();  // generic writes of Eb before later bulk accesses
     __syncthreads();
+    if (store && tid == 0) {
+      bulk_s2g(my_escr + size_t(soff) * n, Eb, unsigned(m) * unsigned(n) * 4u);
+      bulk_commit();
+    }
+    return true;
+  };
+  // Waits (thread 0) for the records in ring slot r3 and makes them visible.
+  auto records_ready = [&](int r3) -> bool {
+    if (tid == 0 && !failed && !wait_bar(r3)) failed = true;
+    if (__syncthreads_or(tid == 0 && failed)) {
+      if (tid == 0) atomicCAS(&bar->err, DEVERR_NONE, DEVERR_TIMEOUT);
+      return false;
+    }
+    return true;
   };
 
   float blk[TN][TN];
@@ -305,16 +396,38 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
     // ---- phase A: partial Gram of this CTA's residual columns -------------
     const int sb = int(int64_t(c_eff) * b / active), se = int(int64_t(c_eff) * (b + 1) / active);
     const bool in_a = b < active;
+    const int nch = in_a ? (se - sb + kEChunk - 1) / kEChunk : 0;
+    const bool resident = nch == 1;
     if (in_a) {
 #pragma unroll
       for (int r = 0; r < TN; ++r)
 #pragma unroll
-        for (int s = 0; s < TN; ++s) blk[r][s] = 0.0f;
-      for (int t0 = sb; t0 < se; t0 += kEChunk) {
+        for (int s2 = 0; s2 < TN; ++s2) blk[r][s2] = 0.0f;
+      lap(0);
+      float cfv[kCfRegs];
+      issue_records(beg, sb, min(kEChunk, se - sb), 0);
+      if (nch > 1) issue_records(beg, sb + kEChunk, min(kEChunk, se - sb - kEChunk), 1);
+      if (!records_ready(0)) return;
+      issue_patches(min(kEChunk, se - sb), 0, 0, true);
+      gather_load(min(kEChunk, se - sb), 0, cfv);
+      gather_store(min(kEChunk, se - sb), 0, cfv);
+      lap(11);
+      for (int ch = 0; ch < nch; ++ch) {
+        const int buf = ch & 1, r3 = ch % 3;
+        const int t0 = sb + ch * kEChunk;
         const int m = min(kEChunk, se - t0);
-        build_chunk(beg, t0, m);
+        const int m1 = min(kEChunk, se - t0 - kEChunk);  // next chunk (if any)
+        if (ch + 1 < nch) issue_patches(m1, (ch + 1) % 3, buf ^ 1, false);
+        if (ch + 2 < nch) issue_records(beg, t0 + 2 * kEChunk, min(kEChunk, se - t0 - 2 * kEChunk), (ch + 2) % 3);
+        lap(11);
+        if (!finish(m, r3, buf, !resident && tma, t0 - sb)) return;
+        lap(12);
+        // the next chunk's records are visible now (waited above, synced in
+        // finish): prefetch its coefficients while this chunk accumulates
+        if (ch + 1 < nch) gather_load(m1, (ch + 1) % 3, cfv);
+        const float* Eb = Ebase + size_t(buf) * kEChunk * n;
         for (int q = 0; q < m; ++q) {
-          const float* er = E + q * n;
+          const float* er = Eb + q * n;
           float ra[TN], rb[TN];
 #pragma unroll
           for (int r = 0; r < TN; ++r) {
@@ -322,24 +435,27 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
             ra[r] = (i < n) ? er[i] : 0.0f;
           }
 #pragma unroll
-          for (int s = 0; s < TN; ++s) {
-            const int k = tj + 16 * s;
-            rb[s] = (k < n) ? er[k] : 0.0f;
+          for (int s2 = 0; s2 < TN; ++s2) {
+            const int k = tj + 16 * s2;
+            rb[s2] = (k < n) ? er[k] : 0.0f;
           }
 #pragma unroll
           for (int r = 0; r < TN; ++r)
 #pragma unroll
-            for (int s = 0; s < TN; ++s) blk[r][s] = fmaf(ra[r], rb[s], blk[r][s]);
+            for (int s2 = 0; s2 < TN; ++s2) blk[r][s2] = fmaf(ra[r], rb[s2], blk[r][s2]);
         }
-        if (t0 + kEChunk < se) __syncthreads();  // E is rebuilt by the next chunk
+        if (ch + 1 < nch) gather_store(m1, buf ^ 1, cfv);
+        fence_proxy_async_smem();
+        __syncthreads();
+        lap(13);
       }
       float* gp = gpart + size_t(b) * nn;
 #pragma unroll
       for (int r = 0; r < TN; ++r)
 #pragma unroll
-        for (int s = 0; s < TN; ++s) {
-          const int i = ti + 16 * r, k = tj + 16 * s;
-          if (i < n && k < n) gp[i * n + k] = blk[r][s];
+        for (int s2 = 0; s2 < TN; ++s2) {
+          const int i = ti + 16 * r, k = tj + 16 * s2;
+          if (i <= k && k < n) gp[i * n + k] = blk[r][s2];
         }
     }
     __syncthreads();
@@ -351,9 +467,20 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
     {
       const int qb = int(int64_t(nn) * b / G), qe = int(int64_t(nn) * (b + 1) / G);
       for (int q = qb + tid; q < qe; q += kUpdThreads) {
-        float s = 0.0f;
-        for (int bb = 0; bb < active; ++bb) s += __ldcg(gpart + size_t(bb) * nn + q);
-        gsum[q] = s;
+        const int i = q / n, k = q - i * n;
+        if (i > k) continue;
+        float s0 = 0.0f, s1 = 0.0f, s2 = 0.0f, s3 = 0.0f;
+        int bb = 0;
+        for (; bb + 3 < active; bb += 4) {
+          s0 += __ldcg(gpart + size_t(bb) * nn + q);
+          s1 += __ldcg(gpart + size_t(bb + 1) * nn + q);
+          s2 += __ldcg(gpart + size_t(bb + 2) * nn + q);
+          s3 += __ldcg(gpart + size_t(bb + 3) * nn + q);
+        }
+        for (; bb < active; ++bb) s0 += __ldcg(gpart + size_t(bb) * nn + q);
+        const float v = (s0 + s1) + (s2 + s3);
+        gsum[q] = v;
+        gsum[k * n + i] = v;  // both triangles: phase C reads rows contiguously
       }
     }
     __syncthreads();
@@ -365,22 +492,23 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
 #pragma unroll
     for (int r = 0; r < TN; ++r)
 #pragma unroll
-      for (int s = 0; s < TN; ++s) {
-        const int i = ti + 16 * r, k = tj + 16 * s;
-        blk[r][s] = (i < n && k < n) ? __ldcg(gsum + i * n + k) : 0.0f;
+      for (int s2 = 0; s2 < TN; ++s2) {
+        const int i = ti + 16 * r, k = tj + 16 * s2;
+        blk[r][s2] = (i < n && k < n) ? __ldcg(gsum + i * n + k) : 0.0f;
       }
     for (int i = tid; i < npad; i += kUpdThreads) u[i] = dold[i];
     __syncthreads();
+    lap(14);
     int iters = 0;
     for (int it = 0; it < kMaxPowerIters; ++it) {
       float ub[TN], v[TN];
 #pragma unroll
-      for (int s = 0; s < TN; ++s) ub[s] = u[tj + 16 * s];
+      for (int s2 = 0; s2 < TN; ++s2) ub[s2] = u[tj + 16 * s2];
 #pragma unroll
       for (int r = 0; r < TN; ++r) {
         float acc = 0.0f;
 #pragma unroll
-        for (int s = 0; s < TN; ++s) acc = fmaf(blk[r][s], ub[s], acc);
+        for (int s2 = 0; s2 < TN; ++s2) acc = fmaf(blk[r][s2], ub[s2], acc);
         v[r] = acc;
       }
 #pragma unroll
@@ -425,19 +553,61 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
 
     // ---- coefficients x_{j,p} = u . e_p ------------------------------------
     if (in_a) {
-      const bool resident = (se - sb) <= kEChunk;  // E still holds this CTA's columns
-      for (int t0 = sb; t0 < se; t0 += kEChunk) {
-        const int m = min(kEChunk, se - t0);
-        if (!resident) {
-          __syncthreads();
-          build_chunk(beg, t0, m);
-        }
+      auto dots = [&](int buf, int t0, int m) {
+        const float* Eb = Ebase + size_t(buf) * kEChunk * n;
         for (int q = warp; q < m; q += kUpdThreads / 32) {
-          const float* er = E + q * n;
+          const float* er = Eb + q * n;
           float dp = 0.0f;
           for (int i = lane; i < n; i += 32) dp = fmaf(u[i], er[i], dp);
           dp = warp_sum(dp);
-          if (lane == 0) coef[int64_t(mp[q]) * L + ms[q]] = dp;
+          if (lane == 0) coef[__ldg(entries + beg + t0 + q)] = dp;
+        }
+      };
+      if (resident) {
+        dots(0, sb, se - sb);  // buffer 0 still holds this CTA's columns
+        fence_proxy_async_smem();
+      } else if (!tma) {
+        // rows not 16-byte aligned: rebuild the columns (generic loads)
+        issue_records(beg, sb, min(kEChunk, se - sb), 0);
+        for (int ch = 0; ch < nch; ++ch) {
+          const int buf = ch & 1, r3 = ch % 3;
+          const int t0 = sb + ch * kEChunk;
+          const int m = min(kEChunk, se - t0);
+          if (ch + 1 < nch) issue_records(beg, t0 + kEChunk, min(kEChunk, se - t0 - kEChunk), (ch + 1) % 3);
+          if (!records_ready(r3)) return;
+          float cfv[kCfRegs];
+          gather_load(m, r3, cfv);
+          gather_store(m, buf, cfv);
+          if (!finish(m, r3, buf, false, 0)) return;
+          dots(buf, t0, m);
+          __syncthreads();
+        }
+      } else {
+        // stream the columns back from the scratch
+        if (tid == 0) bulk_wait0();  // this CTA's scratch stores are complete
+        auto issue_cols = [&](int ch) {
+          if (tid == 0 && !failed) {
+            const int t0 = sb + ch * kEChunk, m = min(kEChunk, se - t0), buf = ch & 1;
+            mbar_arrive_expect_tx(&bars[3 + buf], unsigned(m) * unsigned(n) * 4u);
+            bulk_g2s(Ebase + size_t(buf) * kEChunk * n, my_escr + size_t(t0 - sb) * n, unsigned(m) * unsigned(n) * 4u,
+                     &bars[3 + buf]);
+          }
+        };
+        __syncthreads();  // the scratch is complete before it is read back
+        issue_cols(0);
+        for (int ch = 0; ch < nch; ++ch) {
+          const int buf = ch & 1;
+          const int t0 = sb + ch * kEChunk;
+          const int m = min(kEChunk, se - t0);
+          if (ch + 1 < nch) issue_cols(ch + 1);
+          const bool ok = wait_bar(3 + buf);
+          if (__syncthreads_or(!ok || (tid == 0 && failed))) {
+            if (tid == 0) atomicCAS(&bar->err, DEVERR_NONE, DEVERR_TIMEOUT);
+            return;
+          }
+          dots(buf, t0, m);
+          fence_proxy_async_smem();
+          __syncthreads();
         }
       }
     }
@@ -450,6 +620,7 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
     if (!grid_sync(bar, G)) return;
     lap(6);
   }
+  if (tid == 0) bulk_wait0();
 }
 
 __global__ void accumulate_phases_kernel(const DevStats* __restrict__ src, DevStats* __restrict__ dst) {
@@ -501,9 +672,16 @@ int update_grid_size(int n, int K, int L, int num_sms) {
   return num_sms;  // one CTA per SM: co-resident by construction
 }
 
+int64_t update_scratch_cap(int64_t N, int grid) {
+  int64_t per = (N + grid - 1) / grid + 1;
+  return per > kMinEntriesPerCta ? per : kMinEntriesPerCta;
+}
+
 cudaError_t launch_update(const float* patches, int64_t N, int n, float* dict, int K, int L, const int32_t* idx,
-                          float* coef, CsrWork w, int q1_cap, float* gpart, float* gsum, GridBarrier* bar,
-                          DevStats* stats, int grid, cudaStream_t s) {
+                          float* coef, CsrWork w, int q1_cap, float* gpart, float* gsum, float* escr,
+                          int64_t escr_cap, GridBarrier* bar, DevStats* stats, int grid, cudaStream_t s) {
+  // bulk copies need 16-byte aligned rows
+  int tma = ((n * 4) % 16 == 0 && (reinterpret_cast<uintptr_t>(patches) & 15) == 0) ? 1 : 0;
   const bool dsmem = dict_in_smem(n, K, L);
   void* fn = pick_update(n, dsmem);
   if (!fn || grid < 1) return cudaErrorInvalidValue;
@@ -514,9 +692,11 @@ cudaError_t launch_update(const float* patches, int64_t N, int n, float* dict, i
   if (e != cudaSuccess) return e;
   const int* atom_ptr = w.atom_ptr;
   const int* entries = w.entries;
-  void* args[] = {(void*)&patches, (void*)&N,       (void*)&n,       (void*)&dict,     (void*)&K,
-                  (void*)&L,       (void*)&idx,     (void*)&coef,    (void*)&atom_ptr, (void*)&entries,
-                  (void*)&q1_cap,  (void*)&gpart,   (void*)&gsum,    (void*)&bar,      (void*)&stats};
+  const int* records = w.records;
+  void* args[] = {(void*)&patches, (void*)&N,     (void*)&n,       (void*)&dict,     (void*)&K,
+                  (void*)&L,       (void*)&idx,   (void*)&coef,    (void*)&atom_ptr, (void*)&entries,
+                  (void*)&records, (void*)&q1_cap, (void*)&tma,    (void*)&gpart,    (void*)&gsum,
+                  (void*)&escr,    (void*)&escr_cap, (void*)&bar,  (void*)&stats};
   return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kUpdThreads), args, smem, s);
 }
 

@@ -72,13 +72,23 @@ cudaError_t launch_omp_fp32(const float* patches, int64_t N, int n, const float*
                             int K, int L, int32_t* idx, float* coef, int num_sms, DevStats* stats,
                             cudaStream_t s);
 
+// OMP with the BF16 tensor-core correlation and exact FP32/FP64 re-scoring.
+size_t omp_tc_smem_bytes(int n, int K, int L);
+bool omp_tc_supported(int n, int K, int L);
+cudaError_t launch_omp_tc(const float* patches, int64_t N, int n, const float* dict, const double* gram, int K,
+                          int L, int32_t* idx, float* coef, int num_sms, GridBarrier* flags, DevStats* stats,
+                          cudaStream_t s);
+
 // Dictionary update.
 struct CsrWork {
   int* chunk_counts;   // nchunks x K
-  int* atom_ptr;       // K + 1
+  int* atom_ptr;       // 2K + 1 (atom_ptr[0..K], then scratch)
   int* entries;        // N * L (patch * L + slot), grouped by atom, ascending patch
+  int* records;        // N * L records of csr_record_ints(L) ints, same order:
+                       // {patch, slot, atom of slot 0..L-1 (-1 if unused), pad}
   int64_t nchunks;
 };
+inline int csr_record_ints(int L) { return (L + 2 + 3) / 4 * 4; }
 int64_t csr_num_chunks(int64_t N);
 cudaError_t launch_csr_build(const int32_t* idx, const float* coef, int64_t N, int L, int K, CsrWork w,
                              cudaStream_t s);
@@ -86,9 +96,12 @@ bool update_supported(int n);
 cudaError_t launch_accumulate_phases(const DevStats* src, DevStats* dst, cudaStream_t s);
 size_t update_smem_bytes(int n, int K, int L);
 int update_grid_size(int n, int K, int L, int num_sms);
+// Residual-column scratch: grid x cap x n floats, cap = update_scratch_cap(N, grid).
+int64_t update_scratch_cap(int64_t N, int grid);
 cudaError_t launch_update(const float* patches, int64_t N, int n, float* dict, int K, int L,
                           const int32_t* idx, float* coef, CsrWork w, int q1_cap, float* gpart,
-                          float* gsum, GridBarrier* bar, DevStats* stats, int grid, cudaStream_t s);
+                          float* gsum, float* escr, int64_t escr_cap, GridBarrier* bar, DevStats* stats,
+                          int grid, cudaStream_t s);
 
 // Image rebuild.
 cudaError_t launch_col2im(const float* noisy, const PatchGeom& g, const float* dict, int K, int L,

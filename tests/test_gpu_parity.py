@@ -75,13 +75,14 @@ def support_agreement(i1, i2):
     return float(np.mean(np.all(i1 == i2, axis=1)))
 
 
+@pytest.mark.parametrize("precision", [0, 1])
 @pytest.mark.parametrize("K,L", [(64, 5), (32, 3), (256, 5), (100, 8)])
-def test_omp_vs_fp64_oracle(torch_cuda, ksvd, oracle, case, K, L):
+def test_omp_vs_fp64_oracle(torch_cuda, ksvd, oracle, case, K, L, precision):
     _, noisy = case
     Y = oracle.extract_patches(noisy, 8, 8, 2, 2)
     D = oracle.init_dictionary(Y, K, int_norm=True, dtype=np.float32)
     idx, coef = run_omp(torch_cuda, ksvd, Y, D, patch_width_dim=8, patch_height_dim=8, sliding_width=2,
-                        sliding_height=2, atoms=K, omp_iter=L)
+                        sliding_height=2, atoms=K, omp_iter=L, precision=precision)
     ri, rc = oracle.omp(Y.astype(np.float64), D.astype(np.float64), L)
     agree = support_agreement(idx, ri)
     assert agree >= 0.999, agree
@@ -90,7 +91,26 @@ def test_omp_vs_fp64_oracle(torch_cuda, ksvd, oracle, case, K, L):
     assert rel.max() < 1e-4, rel.max()
 
 
-def test_omp_edge_cases(torch_cuda, ksvd, oracle):
+@pytest.mark.parametrize("precision", [0, 1])
+def test_omp_img512_patches(torch_cuda, ksvd, oracle, synth, precision):
+    """12x12 patches of the 512^2 workload image (27,889 patches, 144-dim),
+    256 atoms, L = 5: support agreement with the FP64 oracle >= 99.9%."""
+    w = synth.WORKLOADS["img512_p12s3_k256"]
+    _, noisy = w.images()
+    Y = oracle.extract_patches(noisy, 12, 12, 3, 3)
+    D = oracle.init_dictionary(Y, 256, int_norm=True, dtype=np.float32)
+    idx, coef = run_omp(torch_cuda, ksvd, Y, D, patch_width_dim=12, patch_height_dim=12, sliding_width=3,
+                        sliding_height=3, atoms=256, omp_iter=5, precision=precision)
+    ri, rc = oracle.omp(Y.astype(np.float64), D.astype(np.float64), 5)
+    agree = support_agreement(idx, ri)
+    assert agree >= 0.999, agree
+    m = np.all(idx == ri, axis=1)
+    rel = np.abs(coef[m] - rc[m]) / (np.abs(rc[m]).max(axis=1, keepdims=True) + 1e-30)
+    assert rel.max() < 1e-4, rel.max()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_omp_edge_cases(torch_cuda, ksvd, oracle, precision):
     # zero patches, exactly representable patches, fewer patches than a tile
     r = np.random.default_rng(5)
     D = r.normal(size=(40, 64)).astype(np.float32)
@@ -99,7 +119,8 @@ def test_omp_edge_cases(torch_cuda, ksvd, oracle):
     Y[1] = 3.0 * D[7]
     Y[2] = 2.0 * D[3] - 1.0 * D[11]
     Y[3:] = r.normal(scale=50.0, size=(34, 64))
-    idx, coef = run_omp(torch_cuda, ksvd, Y, D, patch_width_dim=8, patch_height_dim=8, atoms=40, omp_iter=5)
+    idx, coef = run_omp(torch_cuda, ksvd, Y, D, patch_width_dim=8, patch_height_dim=8, atoms=40, omp_iter=5,
+                        precision=precision)
     ri, rc = oracle.omp(Y.astype(np.float64), D.astype(np.float64), 5)
     assert list(idx[0]) == [0, -1, -1, -1, -1] and coef[0, 0] == 0.0
     assert idx[1, 0] == 7 and abs(coef[1, 0] - 3.0) < 1e-5
@@ -201,12 +222,13 @@ def test_codes_to_dense(torch_cuda, ksvd, oracle, case, geo):
     np.testing.assert_array_equal(dense.cpu().numpy(), ref)
 
 
+@pytest.mark.parametrize("precision", [0, 1])
 @pytest.mark.parametrize("compat,q1", [(1, False), (3, True)])
-def test_denoise_psnr_vs_fp64_oracle(torch_cuda, ksvd, oracle, synth, compat, q1):
+def test_denoise_psnr_vs_fp64_oracle(torch_cuda, ksvd, oracle, synth, compat, q1, precision):
     clean = synth.clean_image(128, 31)
     noisy = synth.add_gaussian(clean, 20.0, 31)
     kw = dict(patch_width_dim=8, patch_height_dim=8, sliding_width=2, sliding_height=2, atoms=64, omp_iter=5,
-              ksvd_iter=4, compat=compat)
+              ksvd_iter=4, compat=compat, precision=precision)
     with mkctx(ksvd, **kw) as c:
         out, st = c.denoise(noisy, 400.0)
     ref, info = oracle.ksvd_denoise(noisy, 400.0, pw=8, ph=8, sw=2, sh=2, atoms=64, ksvd_iter=4, omp_iter=5,
@@ -260,13 +282,14 @@ def test_zero_image_reports_zero_atom(torch_cuda, ksvd):
 
 
 @pytest.mark.slow
-def test_denoise_img512_workload_vs_fp64_oracle(torch_cuda, ksvd, oracle, synth):
+@pytest.mark.parametrize("precision", [0, 1])
+def test_denoise_img512_workload_vs_fp64_oracle(torch_cuda, ksvd, oracle, synth, precision):
     """The 512^2 workload (sigma 20, 12x12 stride 3, 256 atoms, L=5, 10
     iterations), reference-compatible mode, against the FP64 oracle."""
     w = synth.WORKLOADS["img512_p12s3_k256"]
     clean, noisy = w.images()
     kw = dict(patch_width_dim=12, patch_height_dim=12, sliding_width=3, sliding_height=3, atoms=256, omp_iter=5,
-              ksvd_iter=10, compat=3)
+              ksvd_iter=10, compat=3, precision=precision)
     with mkctx(ksvd, **kw) as c:
         out, st = c.denoise(noisy, w.sigma ** 2)
     ref, _ = oracle.ksvd_denoise(noisy, w.sigma ** 2, pw=12, ph=12, sw=3, sh=3, atoms=256, ksvd_iter=10,
