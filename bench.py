@@ -200,7 +200,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="img2048_p12s3_k256")
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16", "fp16"])
     ap.add_argument("--compat", type=int, default=1, help="KSVD_COMPAT_* bits (1 = INT_NORM, 3 = +Q1 cap)")
     ap.add_argument("--e2e-calls", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -223,7 +223,7 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
 
     ksvd = pkg.ksvd
-    prec = ksvd.PREC_FP32 if args.precision == "fp32" else ksvd.PREC_BF16_RESCORE
+    prec = {"fp32": ksvd.PREC_FP32, "bf16": ksvd.PREC_BF16_RESCORE, "fp16": ksvd.PREC_FP16_RESCORE}[args.precision]
     params = ksvd.make_params(patch_width_dim=wl.patch, patch_height_dim=wl.patch, sliding_width=wl.stride,
                               sliding_height=wl.stride, atoms=wl.atoms, omp_iter=wl.omp_iter,
                               ksvd_iter=wl.ksvd_iter, precision=prec, compat=args.compat, device=local)
@@ -277,6 +277,7 @@ def main():
     gpu_launches = ctx.launch_count() - launches0
     fam = {f: ctx.profile_read(f) for f in ("gram", "omp", "csr", "update")}
     phases = ctx.profile_phases()
+    counters = ctx.profile_counters()
     ctx.profile(False)
     ms_step = ms_total / args.steps
     if dist:
@@ -337,7 +338,8 @@ def main():
         line = {
             "metric": "patches/s per K-SVD iteration", "value": value, "unit": "patches/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else "bf16+f32",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": {"fp32": "f32", "bf16": "bf16+f32", "fp16": "f16+f32"}[args.precision],
             "data": "synthetic",
             "config": {"workload": wl.name, "image": f"{wl.size}x{wl.size}", "sigma": wl.sigma,
                        "patch": f"{wl.patch}x{wl.patch}", "stride": wl.stride, "num_patches": N, "atoms": K,
@@ -357,6 +359,7 @@ def main():
                     (0, "upd_gram"), (1, "upd_wait1"), (2, "upd_sum"), (3, "upd_wait2"), (4, "upd_power"),
                     (5, "upd_coef"), (6, "upd_wait3"), (8, "omp_corr"), (9, "omp_ls"), (10, "omp_io"),
                     (11, "upd_gram_stage"), (12, "upd_gram_finish"), (13, "upd_gram_acc"), (14, "upd_gload"))},
+            "counters_per_step": {k: v / max(args.steps, 1) for k, v in counters.items()},
             "quality": {"psnr_noisy": psnr_noisy, "psnr_denoised": psnr_out,
                         "power_iters_last_sweep": st.power_iters, "atoms_updated_last_sweep": st.atoms_updated},
             "clocks": clocks.summary(),

@@ -142,7 +142,9 @@ ksvd_status validate_params(const ksvd_params* p, std::string* why) {
   if (p->omp_iter < 1 || p->omp_iter > 32) return bad("ompIter must be in [1, 32]");
   if (p->ksvd_iter < 0) return bad("ksvdIter must be >= 0");
   if (p->type < KSVD_CUDA_K_GESVD || p->type > KSVD_CUDA_K_SM100A) return bad("unknown type");
-  if (p->precision != KSVD_PREC_FP32 && p->precision != KSVD_PREC_BF16_RESCORE) return bad("unknown precision");
+  if (p->precision != KSVD_PREC_FP32 && p->precision != KSVD_PREC_BF16_RESCORE &&
+      p->precision != KSVD_PREC_FP16_RESCORE)
+    return bad("unknown precision");
   if (p->sub_image_width_dim < 0 || p->sub_image_height_dim < 0) return bad("sub-image dimensions must be >= 0");
   return KSVD_OK;
 }
@@ -338,6 +340,18 @@ ksvd_status ksvd_profile_read(ksvd_ctx* c, const char* family, double* total_ms,
 
 int64_t ksvd_launch_count(const ksvd_ctx* c) { return c ? c->launch_count : 0; }
 
+ksvd_status ksvd_profile_counters(ksvd_ctx* c, int64_t* out, int count) {
+  if (!c || !out || count < 1) return KSVD_ERR_INVALID;
+  KSVD_TRY(check_ctx(c));
+  ksvd::DevStats h{};
+  KSVD_CU(c, cudaStreamSynchronize(c->stream), "profile sync");
+  KSVD_CU(c, cudaMemcpy(&h, c->d_phase, sizeof(h), cudaMemcpyDeviceToHost), "counters");
+  const int64_t v[4] = {int64_t(h.power_iters), int64_t(h.atoms_updated), int64_t(h.omp_rescore_misses),
+                        int64_t(h.pad)};
+  for (int i = 0; i < count; ++i) out[i] = i < 4 ? v[i] : 0;
+  return KSVD_OK;
+}
+
 ksvd_status ksvd_profile_phases(ksvd_ctx* c, double* ms_out, int count) {
   if (!c || !ms_out || count < 1) return KSVD_ERR_INVALID;
   KSVD_TRY(check_ctx(c));
@@ -387,9 +401,10 @@ static ksvd_status omp_impl(ksvd_ctx* c, const float* d_patches, int64_t N, cons
     KSVD_CU(c, ksvd::launch_gram_f64(d_dict, K, n, gram, c->stream), "gram");
   }
   Prof pr(c, "omp", 1);
-  if (c->p.precision == KSVD_PREC_BF16_RESCORE) {
+  if (c->p.precision != KSVD_PREC_FP32) {
     KSVD_CU(c,
-            ksvd::launch_omp_tc(d_patches, N, n, d_dict, gram, K, L, d_idx, d_coef, c->num_sms, c->d_flags,
+            ksvd::launch_omp_tc(d_patches, N, n, d_dict, gram, K, L, d_idx, d_coef, c->num_sms,
+                                c->p.precision == KSVD_PREC_FP16_RESCORE ? 1 : 0, c->d_flags,
                                 c->profiling ? c->d_phase : nullptr, c->stream),
             "omp (tensor cores)");
   } else {
@@ -407,7 +422,7 @@ ksvd_status ksvd_omp(ksvd_ctx* c, const float* d_patches, int64_t N, const float
   if (!d_patches || !d_dict || !d_idx || !d_coef || N < 1) return fail(c, KSVD_ERR_INVALID, "bad argument");
   KSVD_TRY(check_kernel_support(c));
   KSVD_TRY(omp_impl(c, d_patches, N, d_dict, d_idx, d_coef));
-  if (c->p.precision == KSVD_PREC_BF16_RESCORE) return check_dev_flags(c, "omp");
+  if (c->p.precision != KSVD_PREC_FP32) return check_dev_flags(c, "omp");
   return KSVD_OK;
 }
 

@@ -19,6 +19,7 @@
 //     norm (:352-393; stop when below 1e-3, :218) and writes the residual as
 //     BF16 into the A operand of the next step.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "device_util.cuh"
@@ -27,15 +28,72 @@
 namespace ksvd {
 
 constexpr int kTcTile = 128;     // patches per tile = UMMA M = TMEM lanes
-constexpr int kTcThreads = 128;  // one epilogue thread per patch
-constexpr int kTopT = 8;         // BF16 candidates re-scored exactly
+constexpr int kTcQ = 4;          // threads per patch (column quarters)
+constexpr int kTcThreads = kTcTile * kTcQ;
+// |c_tc - c| / (|r| |d|): both operands rounded to p-bit significands (2 x
+// 2^-p) plus FP32 accumulation and subnormal slack.
+constexpr float kErrBf16 = 2.0f / 256.0f + 4.0e-4f;
+constexpr float kErrF16 = 2.0f / 2048.0f + 1.0e-4f;
+
+// 16-bit operand element: BF16 (8-bit significand) or FP16 (11-bit).
+template <bool F16>
+struct Op16;
+template <>
+struct Op16<false> {
+  static __device__ __forceinline__ unsigned short cvt(float x) {
+    return __bfloat16_as_ushort(__float2bfloat16_rn(x));
+  }
+  static constexpr unsigned fmt = 1u;  // instruction-descriptor format code
+  static constexpr float err = kErrBf16;
+};
+template <>
+struct Op16<true> {
+  static __device__ __forceinline__ unsigned short cvt(float x) { return __half_as_ushort(__float2half_rn(x)); }
+  static constexpr unsigned fmt = 0u;
+  static constexpr float err = kErrF16;
+};
+
+__device__ __forceinline__ void store8(unsigned char* dst, const unsigned short (&h)[8]) {
+  uint4 v;
+  v.x = unsigned(h[0]) | (unsigned(h[1]) << 16);
+  v.y = unsigned(h[2]) | (unsigned(h[3]) << 16);
+  v.z = unsigned(h[4]) | (unsigned(h[5]) << 16);
+  v.w = unsigned(h[6]) | (unsigned(h[7]) << 16);
+  *reinterpret_cast<uint4*>(dst) = v;
+}
+
+// Power of two 2^e with max_abs * 2^-e in [2^13, 2^14) (1 for max_abs == 0):
+// scaling the A operand by 2^-e is exact and keeps FP16 far from overflow and
+// from its subnormal range.
+__device__ __forceinline__ float pow2_scale(float max_abs) {
+  if (!(max_abs > 0.0f)) return 1.0f;
+  int e;
+  frexpf(max_abs, &e);  // max_abs = f * 2^e, f in [0.5, 1)
+  return ldexpf(1.0f, e - 14);
+}
 constexpr int kTcLMax = 16;
 constexpr unsigned long long kMmaWaitNs = 2000000000ull;
 
 struct TcLayout {
-  int Kp, np16, ysn, tri;
-  size_t off_b, off_a, off_y, off_lc, off_bv, off_s, off_gam, off_bar, off_tmem, total;
+  int Kp, np16, ysn, tri, qw;
+  size_t off_b, off_a, off_y, off_lc, off_bv, off_s, off_gam, off_sum, off_pp, off_xq, off_bar, off_tmem, total;
   unsigned tmem_cols;
+};
+
+// Per-patch scalars shared by the patch's four threads.
+struct TcPatch {
+  int cnt, done;
+  float rmean, rscale, rnorm, ysum;
+  double yy;
+};
+
+// Exchange between the four threads of a patch.
+struct TcX {
+  float qmax[kTcQ];                 // largest tensor-core |c| per column quarter
+  unsigned long long qmask[kTcQ];   // columns of each quarter inside the error window
+  float2 part[kTcQ];                // residual partial norms (all, centred)
+  double best, best_b;              // exact best |c| and its d_a . y
+  int best_a, pad;
 };
 
 __host__ __device__ inline size_t tc_al(size_t x, size_t a) { return (x + a - 1) / a * a; }
@@ -61,6 +119,12 @@ __host__ __device__ inline TcLayout tc_layout(int n, int K, int L) {
   off = tc_al(off + size_t(kTcTile) * L * 4, 16);
   o.off_gam = off;
   off = tc_al(off + size_t(kTcTile) * L * 4, 16);
+  o.off_sum = off;
+  off = tc_al(off + size_t(o.Kp) * 4, 16);
+  o.off_pp = off;
+  off = tc_al(off + size_t(kTcTile) * sizeof(TcPatch), 16);
+  o.off_xq = off;
+  off = tc_al(off + size_t(kTcTile) * sizeof(TcX), 16);
   o.off_bar = off;
   off = tc_al(off + 16, 16);
   o.off_tmem = off;
@@ -69,6 +133,7 @@ __host__ __device__ inline TcLayout tc_layout(int n, int K, int L) {
   unsigned cols = 32;
   while (cols < unsigned(o.Kp)) cols <<= 1;
   o.tmem_cols = cols;
+  o.qw = int(tc_al((o.Kp + kTcQ - 1) / kTcQ, 16));  // columns per quarter, 16-column loads
   return o;
 }
 
@@ -89,11 +154,12 @@ __device__ __forceinline__ unsigned long long umma_desc(unsigned saddr, unsigned
   return d;          // base offset 0, LBO mode 0, layout type 0 (no swizzle)
 }
 
-// Instruction descriptor: BF16 x BF16 -> FP32, A and B K-major, M x N.
-__host__ __device__ constexpr unsigned umma_idesc_bf16(int M, int N) {
+// Instruction descriptor: 16-bit x 16-bit -> FP32 (fmt: 0 = F16, 1 = BF16),
+// A and B K-major, M x N.
+__host__ __device__ constexpr unsigned umma_idesc_16(int M, int N, unsigned fmt) {
   return (1u << 4)                       // D format F32
-         | (1u << 7)                     // A format BF16
-         | (1u << 10)                    // B format BF16
+         | (fmt << 7)                    // A format
+         | (fmt << 10)                   // B format
          | (unsigned(N >> 3) << 17)      // N / 8
          | (unsigned(M >> 4) << 24);     // M / 16
 }
@@ -115,6 +181,20 @@ KSVD_DEV void tc_commit(unsigned long long* bar) {
                : "memory");
 }
 
+// 16 consecutive FP32 columns of this thread's TMEM lane.
+KSVD_DEV void tc_ld16(unsigned taddr, float (&v)[16]) {
+  unsigned r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+KSVD_DEV void tc_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
 // 32 consecutive FP32 columns of this thread's TMEM lane.
 KSVD_DEV void tc_ld32(unsigned taddr, float (&v)[32]) {
   unsigned r[32];
@@ -131,6 +211,7 @@ KSVD_DEV void tc_ld32(unsigned taddr, float (&v)[32]) {
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+template <bool F16>
 __global__ void __launch_bounds__(kTcThreads, 1)
     omp_tc_kernel(const float* __restrict__ Y, int64_t N, int n, const float* __restrict__ D,
                   const double* __restrict__ Gram, int K, int L, int32_t* __restrict__ idx_out,
@@ -144,13 +225,17 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   double* bv = reinterpret_cast<double*>(smem + lo.off_bv);
   int* Ss = reinterpret_cast<int*>(smem + lo.off_s);
   float* gam = reinterpret_cast<float*>(smem + lo.off_gam);
+  float* asum = reinterpret_cast<float*>(smem + lo.off_sum);  // sum_k d_a[k] per atom
+  TcPatch* pp = reinterpret_cast<TcPatch*>(smem + lo.off_pp);
+  TcX* xq = reinterpret_cast<TcX*>(smem + lo.off_xq);
   unsigned long long* mbar = reinterpret_cast<unsigned long long*>(smem + lo.off_bar);
   unsigned* tmem_slot = reinterpret_cast<unsigned*>(smem + lo.off_tmem);
 
-  const int tid = threadIdx.x, warp = tid >> 5;
-  const int Kp = lo.Kp, np16 = lo.np16, ysn = lo.ysn, tri = lo.tri;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int Kp = lo.Kp, np16 = lo.np16, ysn = lo.ysn, tri = lo.tri, qw = lo.qw;
+  const int nkc = np16 / 8;
 
-  // ---- set-up: TMEM, mbarrier, BF16 dictionary operand ---------------------
+  // ---- set-up: TMEM, mbarrier, 16-bit dictionary operand, atom sums --------
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                  "r"(lo.tmem_cols)
@@ -161,56 +246,106 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     mbar_init(mbar, 1);
     fence_mbar_init();
   }
-  for (int t = tid; t < Kp * (np16 / 8); t += kTcThreads) {
-    const int a = t / (np16 / 8), kc = t - a * (np16 / 8);
-    __align__(16) __nv_bfloat16 h[8];
+  for (int t = tid; t < Kp * nkc; t += kTcThreads) {
+    const int a = t / nkc, kc = t - a * nkc;
+    unsigned short h[8];
 #pragma unroll
     for (int e = 0; e < 8; ++e) {
       const int k = kc * 8 + e;
-      h[e] = __float2bfloat16_rn((a < K && k < n) ? __ldg(D + int64_t(a) * n + k) : 0.0f);
+      h[e] = Op16<F16>::cvt((a < K && k < n) ? __ldg(D + int64_t(a) * n + k) : 0.0f);
     }
-    *reinterpret_cast<uint4*>(Bt + canon_off(a, kc * 8, Kp)) = *reinterpret_cast<const uint4*>(h);
+    store8(Bt + canon_off(a, kc * 8, Kp), h);
+  }
+  for (int a = tid; a < Kp; a += kTcThreads) {
+    float sa = 0.0f;
+    if (a < K)
+      for (int k = 0; k < n; ++k) sa += __ldg(D + int64_t(a) * n + k);
+    asum[a] = sa;
   }
   fence_proxy_async_smem();
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const unsigned tmem = *tmem_slot;
-  const unsigned idesc = umma_idesc_bf16(kTcTile, Kp);
+  const unsigned idesc = umma_idesc_16(kTcTile, Kp, Op16<F16>::fmt);
   const unsigned a_base = smem_u32(At), b_base = smem_u32(Bt);
   unsigned phase = 0;
   bool failed = false;
 
-  const int m = tid;  // this thread's patch (and TMEM lane) within a tile
-  const unsigned lane_addr = tmem + (unsigned(warp * 32) << 16);
+  // thread roles: patch m = 32 g + lane (TMEM lane), quarter q of the columns
+  // and of the residual chunks
+  const int g = warp & 3, q = warp >> 2;
+  const int m = g * 32 + lane;
+  const unsigned lane_addr = tmem + (unsigned(g * 32) << 16);
+  const int c_lo = q * qw, c_hi = min(Kp, c_lo + qw);
+  const int kc_lo = (nkc * q) / kTcQ, kc_hi = (nkc * (q + 1)) / kTcQ;
+  TcPatch& P = pp[m];
+  TcX& X = xq[m];
+  const float* yr = Ys + m * ysn;
+  double* Lp = Lc + m * tri;
+  auto Lat = [&](int i, int j) -> double& { return Lp[i * (i + 1) / 2 + j]; };
+
+  const bool timer = (blockIdx.x == 0 && tid == 0 && stats != nullptr);
+  unsigned long long tmark = timer ? globaltimer_ns() : 0ull;
+  auto lap = [&](int slot) {
+    if (timer) {
+      const unsigned long long t = globaltimer_ns();
+      stats->phase_ns[slot] += t - tmark;
+      tmark = t;
+    }
+  };
+  int nscored = 0;
 
   for (int64_t tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
     const int64_t p0 = tile * kTcTile;
     const int np = (N - p0 < kTcTile) ? int(N - p0) : kTcTile;
-    // patch tile: FP32 copy (odd row stride) and the BF16 A operand
     for (int t = tid; t < kTcTile * n; t += kTcThreads) {
       const int p = t / n, k = t - p * n;
       Ys[p * ysn + k] = (p < np) ? __ldg(Y + p0 * n + t) : 0.0f;
     }
     __syncthreads();
-    int cnt = 0;
-    bool done = m >= np;
+    // per-patch sums (quarter 0 thread), then the first A operand row
+    if (q == 0) {
+      float ys = 0.0f;
+      double yy = 0.0;
+      for (int k = 0; k < n; ++k) {
+        ys += yr[k];
+        yy = fma(double(yr[k]), double(yr[k]), yy);
+      }
+      const float mean = ys / float(n);
+      float mx = 0.0f, cc = 0.0f;
+      for (int k = 0; k < n; ++k) {
+        const float c = yr[k] - mean;
+        mx = fmaxf(mx, fabsf(c));
+        cc = fmaf(c, c, cc);
+      }
+      P.cnt = 0;
+      P.done = m >= np;
+      P.ysum = ys;
+      P.yy = yy;
+      P.rmean = mean;
+      P.rscale = pow2_scale(mx);
+      P.rnorm = sqrtf(cc);
+    }
+    __syncthreads();
     {
-      const float* yr = Ys + m * ysn;
-      for (int kc = 0; kc < np16 / 8; ++kc) {
-        __align__(16) __nv_bfloat16 h[8];
+      const float mean = P.rmean, inv = 1.0f / P.rscale;
+      for (int kc = kc_lo; kc < kc_hi; ++kc) {
+        unsigned short h[8];
 #pragma unroll
         for (int e = 0; e < 8; ++e) {
           const int k = kc * 8 + e;
-          h[e] = __float2bfloat16_rn(k < n ? yr[k] : 0.0f);
+          h[e] = Op16<F16>::cvt(k < n ? (yr[k] - mean) * inv : 0.0f);
         }
-        *reinterpret_cast<uint4*>(At + canon_off(m, kc * 8, kTcTile)) = *reinterpret_cast<const uint4*>(h);
+        store8(At + canon_off(m, kc * 8, kTcTile), h);
       }
     }
+    lap(10);
     for (int step = 0; step < L; ++step) {
       fence_proxy_async_smem();
       tc_fence_before();
-      if (!__syncthreads_or(!done)) break;
+      if (!__syncthreads_or(!P.done)) break;
+      lap(9);
       // ---- correlation on the tensor cores ---------------------------------
       if (tid == 0) {
         tc_fence_after();
@@ -230,138 +365,232 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         break;
       }
       tc_fence_after();
-      // ---- top-T candidates by |BF16 correlation| --------------------------
-      float tv[kTopT];
-      int ta[kTopT];
+      lap(8);
+      // ---- this quarter's correlations (tensor part + exact mean part) -----
+      const bool done = P.done != 0;
+      const float rmean = P.rmean, rscale = P.rscale;
+      float cv[64];  // up to 64 columns per quarter (Kp <= 256)
+      float qmax = -1.0f;
+      if (c_lo < Kp) {
 #pragma unroll
-      for (int q = 0; q < kTopT; ++q) {
-        tv[q] = -1.0f;
-        ta[q] = -1;
-      }
-      for (int c0 = 0; c0 < Kp; c0 += 32) {
-        float v[32];
-        tc_ld32(lane_addr + unsigned(c0), v);  // warp-collective: all lanes load
-        if (!done) {
+        for (int j = 0; j < 4; ++j) {
+          if (c_lo + 16 * j < c_hi) {
+            float v[16];
+            tc_ld16(lane_addr + unsigned(c_lo + 16 * j), v);
+            tc_wait_ld();
 #pragma unroll
-          for (int i = 0; i < 32; ++i) {
-            const int a = c0 + i;
-            const float av = fabsf(v[i]);
-            if (a < K && av > tv[kTopT - 1]) {
-              int q = kTopT - 1;
-              while (q > 0 && av > tv[q - 1]) {
-                tv[q] = tv[q - 1];
-                ta[q] = ta[q - 1];
-                --q;
-              }
-              tv[q] = av;
-              ta[q] = a;
+            for (int i = 0; i < 16; ++i) {
+              const int a = c_lo + 16 * j + i;
+              const float c = (a < K) ? fabsf(fmaf(rmean, asum[a], v[i] * rscale)) : -1.0f;
+              cv[16 * j + i] = c;
+              qmax = fmaxf(qmax, c);
             }
           }
         }
       }
-      if (!done) {
-        // ---- exact re-score: c_a = d_a.y - sum_s g_s G[a][s] ----------------
-        const float* yr = Ys + m * ysn;
+      X.qmax[q] = qmax;
+      __syncthreads();
+      // ---- candidates: atoms inside the error window -----------------------
+      // |c_tc - c| <= err |r - rmean 1| |d|, so the exact argmax is among the
+      // atoms with c_tc >= max c_tc - 2 err |r - rmean 1|.
+      {
+        unsigned long long mask = 0ull;
+        if (!done && c_lo < Kp) {
+          float gmax = X.qmax[0];
+#pragma unroll
+          for (int j = 1; j < kTcQ; ++j) gmax = fmaxf(gmax, X.qmax[j]);
+          const float thr = gmax - 2.0f * Op16<F16>::err * P.rnorm;
+#pragma unroll
+          for (int i = 0; i < 64; ++i) {
+            const int a = c_lo + i;
+            if (a < c_hi && a < K && cv[i] >= thr) mask |= 1ull << i;
+          }
+        }
+        X.qmask[q] = mask;
+      }
+      __syncthreads();
+      // ---- exact re-score, four consecutive lanes per patch ----------------
+      //   b_a = d_a . y (FP64 from FP32 data),  c_a = b_a - sum_s g_s G[a][s]
+      {
+        const int ps = tid >> 2, js = tid & 3;
+        const unsigned gmask = 0xFu << (lane & ~3);
+        TcX& XS = xq[ps];
+        const float* yrs = Ys + ps * ysn;
+        const int cnt = pp[ps].cnt;
         double best = -1.0, best_b = 0.0;
-        int best_a = -1;
-        for (int q = 0; q < kTopT; ++q) {
-          const int a = ta[q];
-          if (a < 0) continue;
-          const float4* dr = reinterpret_cast<const float4*>(D + int64_t(a) * n);
-          double ba = 0.0;
-          if (d_vec4) {
-            for (int k4 = 0; k4 < n / 4; ++k4) {
-              const float4 d4 = __ldg(dr + k4);
-              ba = fma(double(d4.x), double(yr[4 * k4]), ba);
-              ba = fma(double(d4.y), double(yr[4 * k4 + 1]), ba);
-              ba = fma(double(d4.z), double(yr[4 * k4 + 2]), ba);
-              ba = fma(double(d4.w), double(yr[4 * k4 + 3]), ba);
+        int best_a = 0x7fffffff;
+        for (int qq = 0; qq < kTcQ; ++qq) {
+          unsigned long long mk = XS.qmask[qq];
+          while (mk) {
+            const int a = qq * qw + (__ffsll((long long)mk) - 1);
+            mk &= mk - 1ull;
+            double b0 = 0.0, b1 = 0.0;
+            if (d_vec4) {
+              const float4* dr = reinterpret_cast<const float4*>(D + int64_t(a) * n);
+              const int n4 = n / 4;
+              for (int k4 = js; k4 < n4; k4 += 4) {
+                const float4 d4 = __ldg(dr + k4);
+                b0 = fma(double(d4.x), double(yrs[4 * k4]), b0);
+                b1 = fma(double(d4.y), double(yrs[4 * k4 + 1]), b1);
+                b0 = fma(double(d4.z), double(yrs[4 * k4 + 2]), b0);
+                b1 = fma(double(d4.w), double(yrs[4 * k4 + 3]), b1);
+              }
+            } else {
+              for (int k = js; k < n; k += 4) b0 = fma(double(__ldg(D + int64_t(a) * n + k)), double(yrs[k]), b0);
             }
-          } else {
-            for (int k = 0; k < n; ++k) ba = fma(double(__ldg(D + int64_t(a) * n + k)), double(yr[k]), ba);
-          }
-          double ca = ba;
-          for (int s = 0; s < cnt; ++s) ca -= double(gam[m * L + s]) * Gram[int64_t(a) * K + Ss[m * L + s]];
-          const double aca = fabs(ca);
-          if (aca > best || (aca == best && a < best_a)) {
-            best = aca;
-            best_a = a;
-            best_b = ba;
+            double ba = b0 + b1;
+            ba += __shfl_xor_sync(gmask, ba, 1);
+            ba += __shfl_xor_sync(gmask, ba, 2);
+            double ca = ba;
+            for (int s2 = 0; s2 < cnt; ++s2) ca -= double(gam[ps * L + s2]) * Gram[int64_t(a) * K + Ss[ps * L + s2]];
+            const double aca = fabs(ca);
+            if (js == 0) ++nscored;
+            if (aca > best || (aca == best && a < best_a)) {
+              best = aca;
+              best_a = a;
+              best_b = ba;
+            }
           }
         }
-        const int a = best_a < 0 ? 0 : best_a;
+        if (js == 0) {
+          XS.best = best;
+          XS.best_a = best_a;
+          XS.best_b = best_b;
+        }
+      }
+      __syncthreads();
+      lap(11);
+      // ---- quarter 0: selection, Cholesky append, solve, residual scale ----
+      if (q == 0 && !done) {
+        const double bbb = X.best_b;
+        const int ba = X.best_a;
+        const int a = (ba >= 0 && ba < K) ? ba : 0;
+        const int k = P.cnt;
         bool stop = false;
-        for (int s = 0; s < cnt; ++s)
-          if (Ss[m * L + s] == a) stop = true;  // re-selected atom: the pursuit ends
+        for (int s2 = 0; s2 < k; ++s2)
+          if (Ss[m * L + s2] == a) stop = true;  // re-selected atom: the pursuit ends
         if (!stop) {
-          // ---- Cholesky row append (packed lower triangle) and solve --------
-          double* Lp = Lc + m * tri;
-          auto Lat = [&](int i, int j) -> double& { return Lp[i * (i + 1) / 2 + j]; };
-          const int k = cnt;
           double ww = 0.0;
           for (int i = 0; i < k; ++i) {
-            double s = Gram[int64_t(Ss[m * L + i]) * K + a];
-            for (int j = 0; j < i; ++j) s -= Lat(i, j) * Lat(k, j);
-            const double wi = s / Lat(i, i);
+            double s3 = Gram[int64_t(Ss[m * L + i]) * K + a];
+            for (int j = 0; j < i; ++j) s3 -= Lat(i, j) * Lat(k, j);
+            const double wi = s3 / Lat(i, i);
             Lat(k, i) = wi;
             ww += wi * wi;
           }
           const double piv2 = Gram[int64_t(a) * K + a] - ww;
           if (!(piv2 > 0.0)) {
-            stop = true;
+            stop = true;  // the new atom depends linearly on the support
           } else {
             Lat(k, k) = sqrt(piv2);
             Ss[m * L + k] = a;
-            bv[m * L + k] = best_b;
-            cnt = k + 1;
+            bv[m * L + k] = bbb;
             double yv[kTcLMax];
             for (int i = 0; i <= k; ++i) {
-              double s = bv[m * L + i];
-              for (int j = 0; j < i; ++j) s -= Lat(i, j) * yv[j];
-              yv[i] = s / Lat(i, i);
+              double s3 = bv[m * L + i];
+              for (int j = 0; j < i; ++j) s3 -= Lat(i, j) * yv[j];
+              yv[i] = s3 / Lat(i, i);
             }
             for (int i = k; i >= 0; --i) {
-              double s = yv[i];
-              for (int j = i + 1; j <= k; ++j) s -= Lat(j, i) * yv[j];
-              yv[i] = s / Lat(i, i);
+              double s3 = yv[i];
+              for (int j = i + 1; j <= k; ++j) s3 -= Lat(j, i) * yv[j];
+              yv[i] = s3 / Lat(i, i);
             }
             for (int i = 0; i <= k; ++i) gam[m * L + i] = float(yv[i]);
+            const int kk = k + 1;
+            P.cnt = kk;
+            // |r|^2 = |y|^2 - 2 g.b + |L^T g|^2 bounds |r - rmean|; mean of
+            // r from the patch sum and the atom sums
+            double rr = P.yy;
+            float rs = P.ysum;
+            for (int i = 0; i < kk; ++i) {
+              rr -= 2.0 * double(gam[m * L + i]) * bv[m * L + i];
+              rs = fmaf(-gam[m * L + i], asum[Ss[m * L + i]], rs);
+            }
+            for (int j = 0; j < kk; ++j) {
+              double z = 0.0;
+              for (int i = j; i < kk; ++i) z += Lat(i, j) * double(gam[m * L + i]);
+              rr += z * z;
+            }
+            P.rmean = rs / float(n);
+            P.rscale = pow2_scale(float(sqrt(fmax(rr, 0.0))) * 1.01f + 1e-30f);
           }
         }
-        if (stop) {
-          done = true;
-        } else {
-          // ---- residual (FP32), its norm, and the next A operand ------------
-          float nrm = 0.0f;
-          for (int kc = 0; kc < np16 / 8; ++kc) {
-            __align__(16) __nv_bfloat16 h[8];
+        if (stop) P.done = 1;
+      }
+      __syncthreads();
+      // ---- residual quarter (FP32), partial norms, next A operand -----------
+      const bool live = !done && !P.done;
+      float nrm = 0.0f, cn = 0.0f;
+      if (live) {
+        const int cnt = P.cnt;
+        const float mean = P.rmean, inv = 1.0f / P.rscale;
+        for (int kc = kc_lo; kc < kc_hi; ++kc) {
+          float r[8];
 #pragma unroll
-            for (int e = 0; e < 8; ++e) {
-              const int kk = kc * 8 + e;
-              float r = 0.0f;
-              if (kk < n) {
-                r = yr[kk];
-                for (int s = 0; s < cnt; ++s) r = fmaf(-gam[m * L + s], __ldg(D + int64_t(Ss[m * L + s]) * n + kk), r);
-                nrm = fmaf(r, r, nrm);
-              }
-              h[e] = __float2bfloat16_rn(r);
-            }
-            *reinterpret_cast<uint4*>(At + canon_off(m, kc * 8, kTcTile)) = *reinterpret_cast<const uint4*>(h);
+          for (int e = 0; e < 8; ++e) {
+            const int kk = kc * 8 + e;
+            r[e] = (kk < n) ? yr[kk] : 0.0f;
           }
-          if (sqrtf(nrm) < 1e-3f) done = true;
+          for (int s2 = 0; s2 < cnt; ++s2) {
+            const float gg = gam[m * L + s2];
+            const float* dr = D + int64_t(Ss[m * L + s2]) * n + kc * 8;
+            if (d_vec4 && kc * 8 + 8 <= n) {
+              const float4 d0 = __ldg(reinterpret_cast<const float4*>(dr));
+              const float4 d1 = __ldg(reinterpret_cast<const float4*>(dr) + 1);
+              r[0] = fmaf(-gg, d0.x, r[0]);
+              r[1] = fmaf(-gg, d0.y, r[1]);
+              r[2] = fmaf(-gg, d0.z, r[2]);
+              r[3] = fmaf(-gg, d0.w, r[3]);
+              r[4] = fmaf(-gg, d1.x, r[4]);
+              r[5] = fmaf(-gg, d1.y, r[5]);
+              r[6] = fmaf(-gg, d1.z, r[6]);
+              r[7] = fmaf(-gg, d1.w, r[7]);
+            } else {
+#pragma unroll
+              for (int e = 0; e < 8; ++e)
+                if (kc * 8 + e < n) r[e] = fmaf(-gg, __ldg(dr + e), r[e]);
+            }
+          }
+          unsigned short h[8];
+#pragma unroll
+          for (int e = 0; e < 8; ++e) {
+            const bool in = kc * 8 + e < n;
+            nrm = fmaf(r[e], r[e], nrm);
+            const float c = in ? r[e] - mean : 0.0f;
+            cn = fmaf(c, c, cn);
+            h[e] = Op16<F16>::cvt(c * inv);
+          }
+          store8(At + canon_off(m, kc * 8, kTcTile), h);
         }
       }
+      float2* part = X.part;
+      part[q] = make_float2(nrm, cn);
+      __syncthreads();
+      if (q == 0 && live) {
+        float tn = 0.0f, tc = 0.0f;
+        for (int j = 0; j < kTcQ; ++j) {
+          tn += part[j].x;
+          tc += part[j].y;
+        }
+        P.rnorm = sqrtf(tc);
+        if (sqrtf(tn) < 1e-3f) P.done = 1;
+      }
+      lap(9);
     }
     // ---- compact codes ------------------------------------------------------
-    if (m < np) {
-      for (int s = 0; s < L; ++s) {
-        const bool used = s < cnt;
-        idx_out[(p0 + m) * L + s] = used ? Ss[m * L + s] : -1;
-        coef_out[(p0 + m) * L + s] = used ? gam[m * L + s] : 0.0f;
+    __syncthreads();
+    if (q == 0 && m < np) {
+      const int cnt = P.cnt;
+      for (int s2 = 0; s2 < L; ++s2) {
+        const bool used = s2 < cnt;
+        idx_out[(p0 + m) * L + s2] = used ? Ss[m * L + s2] : -1;
+        coef_out[(p0 + m) * L + s2] = used ? gam[m * L + s2] : 0.0f;
       }
     }
     __syncthreads();
   }
+  if (stats && nscored) atomicAdd(&stats->pad, (unsigned long long)nscored);
   // ---- teardown --------------------------------------------------------------
   if (failed && tid == 0) mbar_wait(mbar, phase, kMmaWaitNs);  // bounded drain of MMAs in flight
   tc_fence_before();
@@ -370,26 +599,31 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(lo.tmem_cols) : "memory");
   }
-  (void)stats;
 }
 
 size_t omp_tc_smem_bytes(int n, int K, int L) { return tc_layout(n, K, L).total; }
 
+template __global__ void omp_tc_kernel<false>(const float*, int64_t, int, const float*, const double*, int, int,
+                                              int32_t*, float*, int64_t, int, GridBarrier*, DevStats*);
+template __global__ void omp_tc_kernel<true>(const float*, int64_t, int, const float*, const double*, int, int,
+                                             int32_t*, float*, int64_t, int, GridBarrier*, DevStats*);
+
 bool omp_tc_supported(int n, int K, int L) {
-  return L >= 1 && L <= kTcLMax && n >= 1 && K >= 1 && tc_al(K, 16) <= 256 && omp_tc_smem_bytes(n, K, L) <= 227 * 1024;
+  return L >= 1 && L <= kTcLMax && n >= 1 && K >= 1 && tc_al(K, 16) <= 256 &&
+         omp_tc_smem_bytes(n, K, L) <= 232448;
 }
 
 cudaError_t launch_omp_tc(const float* patches, int64_t N, int n, const float* dict, const double* gram, int K, int L,
-                          int32_t* idx, float* coef, int num_sms, GridBarrier* flags, DevStats* stats,
+                          int32_t* idx, float* coef, int num_sms, int fp16, GridBarrier* flags, DevStats* stats,
                           cudaStream_t s) {
   const size_t smem = omp_tc_smem_bytes(n, K, L);
-  cudaError_t e = cudaFuncSetAttribute(omp_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  auto kern = fp16 ? omp_tc_kernel<true> : omp_tc_kernel<false>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   const int64_t ntiles = (N + kTcTile - 1) / kTcTile;
   const int grid = int(std::min<int64_t>(ntiles, num_sms));
   const int d_vec4 = ((n & 3) == 0 && (reinterpret_cast<uintptr_t>(dict) & 15) == 0) ? 1 : 0;
-  omp_tc_kernel<<<grid, kTcThreads, smem, s>>>(patches, N, n, dict, gram, K, L, idx, coef, ntiles, d_vec4, flags,
-                                               stats);
+  kern<<<grid, kTcThreads, smem, s>>>(patches, N, n, dict, gram, K, L, idx, coef, ntiles, d_vec4, flags, stats);
   return cudaGetLastError();
 }
 

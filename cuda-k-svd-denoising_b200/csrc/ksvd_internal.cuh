@@ -34,8 +34,8 @@ struct GridBarrier {
 struct DevStats {
   unsigned long long power_iters;
   unsigned long long atoms_updated;
-  unsigned long long omp_rescore_misses;
-  unsigned long long pad;
+  unsigned long long omp_rescore_misses;  // tensor-core OMP: error windows wider than the candidate list
+  unsigned long long pad;                 // tensor-core OMP: exact re-scores
   // Wall time (ns) CTA 0 spends in each phase of the persistent kernels:
   // update: [0] gram build, [1] wait after it, [2] partial sum, [3] wait,
   // [4] power iteration, [5] coefficients, [6] wait; omp: [8] correlation +
@@ -76,8 +76,8 @@ cudaError_t launch_omp_fp32(const float* patches, int64_t N, int n, const float*
 size_t omp_tc_smem_bytes(int n, int K, int L);
 bool omp_tc_supported(int n, int K, int L);
 cudaError_t launch_omp_tc(const float* patches, int64_t N, int n, const float* dict, const double* gram, int K,
-                          int L, int32_t* idx, float* coef, int num_sms, GridBarrier* flags, DevStats* stats,
-                          cudaStream_t s);
+                          int L, int32_t* idx, float* coef, int num_sms, int fp16, GridBarrier* flags,
+                          DevStats* stats, cudaStream_t s);
 
 // Dictionary update.
 struct CsrWork {

@@ -23,7 +23,7 @@ CUDA_K_GESVD, CUDA_K_GESVDJ, CUDA_K_GESVDA, CUDA_K_SM100A = 0, 1, 2, 3
 OK, ERR_LOAD, ERR_DENOISE, ERR_SAVE = 0, -1, -2, -3
 ERR_INVALID, ERR_CUDA, ERR_NO_MEMORY, ERR_TIMEOUT, ERR_NUMERIC, ERR_NO_DEVICE = -10, -11, -12, -13, -14, -15
 # ksvd_precision
-PREC_FP32, PREC_BF16_RESCORE = 0, 1
+PREC_FP32, PREC_BF16_RESCORE, PREC_FP16_RESCORE = 0, 1, 2
 # compat flags
 COMPAT_INT_NORM, COMPAT_Q1_CAP = 0x1, 0x2
 COMPAT_REFERENCE = COMPAT_INT_NORM | COMPAT_Q1_CAP
@@ -142,6 +142,15 @@ def lib():
         L.ksvd_launch_count.restype = _i64
         L.ksvd_profile_phases.argtypes = [_vp, ctypes.POINTER(ctypes.c_double), _int]
         L.ksvd_profile_phases.restype = _int
+        L.ksvd_profile_counters.argtypes = [_vp, ctypes.POINTER(_i64), _int]
+        L.ksvd_profile_counters.restype = _int
+        L.ksvd_batch_count.argtypes = [ctypes.c_char_p]
+        L.ksvd_batch_count.restype = _int
+        L.ksvd_batch_entry.argtypes = [ctypes.c_char_p, _int, P, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                                       ctypes.c_size_t, ctypes.POINTER(ctypes.c_double)]
+        L.ksvd_batch_entry.restype = _int
+        L.ksvd_run_batch.argtypes = [ctypes.c_char_p, _int]
+        L.ksvd_run_batch.restype = _int
         _lib = L
     return _lib
 
@@ -294,8 +303,39 @@ class Context:
         self._check(lib().ksvd_profile_phases(self.h, arr, 16))
         return list(arr)
 
+    def profile_counters(self) -> dict:
+        arr = (_i64 * 4)()
+        self._check(lib().ksvd_profile_counters(self.h, arr, 4))
+        return {"power_iters": arr[0], "atoms_updated": arr[1], "omp_window_overflows": arr[2],
+                "omp_exact_rescores": arr[3]}
+
     def launch_count(self) -> int:
         return int(lib().ksvd_launch_count(self.h))
+
+
+def batch_config(path: str) -> list[dict]:
+    """Entries of a config.json as the library reads them (BatchDenoiser::factory)."""
+    n = lib().ksvd_batch_count(str(path).encode())
+    if n < 0:
+        raise KsvdError(ERR_INVALID, f"cannot read {path}")
+    out = []
+    for i in range(n):
+        p = KsvdParams()
+        bufs = [ctypes.create_string_buffer(4096) for _ in range(3)]
+        nv = ctypes.c_double(0.0)
+        st = lib().ksvd_batch_entry(str(path).encode(), i, ctypes.byref(p), bufs[0], bufs[1], bufs[2], 4096,
+                                    ctypes.byref(nv))
+        if st != OK:
+            raise KsvdError(st, f"entry {i} of {path}")
+        d = {k: getattr(p, k) for k, _ in p._fields_}
+        d.update(input=bufs[0].value.decode(), output=bufs[1].value.decode(), ref=bufs[2].value.decode(),
+                 noise_variance=nv.value)
+        out.append(d)
+    return out
+
+
+def run_batch(path: str, verbose: bool = False) -> int:
+    return int(lib().ksvd_run_batch(str(path).encode(), int(verbose)))
 
 
 def declared_symbols() -> list[str]:

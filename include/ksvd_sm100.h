@@ -64,10 +64,16 @@ typedef enum ksvd_status {
   KSVD_ERR_NO_DEVICE = -15
 } ksvd_status;
 
-/* Arithmetic of the OMP correlation D^T R. */
+/* Arithmetic of the OMP correlation D^T R.  The tensor-core forms re-score
+ * exactly (FP64 from the FP32 data) every atom whose tensor-core correlation
+ * lies within the operand-rounding error bound of the best one, so the
+ * selected atom is the exact argmax either way; FP16 (11-bit significand,
+ * exact power-of-two scaling per patch) gives an 8x narrower bound than BF16
+ * and therefore far fewer re-scores. */
 typedef enum ksvd_precision {
-  KSVD_PREC_FP32 = 0,        /* plain FP32 FMA                                 */
-  KSVD_PREC_BF16_RESCORE = 1 /* BF16 tensor cores, FP32 re-score of top hits */
+  KSVD_PREC_FP32 = 0,         /* plain FP32 FMA                              */
+  KSVD_PREC_BF16_RESCORE = 1, /* BF16 tensor cores + exact re-score         */
+  KSVD_PREC_FP16_RESCORE = 2  /* FP16 tensor cores + exact re-score         */
 } ksvd_precision;
 
 /* Reference behaviours reproduced on request (bit flags for ksvd_params.compat). */
@@ -207,6 +213,29 @@ int64_t ksvd_launch_count(const ksvd_ctx* ctx);
  * [5] coefficients, [6] grid wait, [8] OMP correlation + argmax, [9] OMP least
  * squares + residual, [10] OMP tile load/store.  Synchronises the stream. */
 ksvd_status ksvd_profile_phases(ksvd_ctx* ctx, double* ms_out, int count);
+/* Counters accumulated while profiling: [0] power iterations, [1] atoms
+ * updated, [2] tensor-core OMP error windows wider than its candidate list,
+ * [3] tensor-core OMP exact re-scores.  Synchronises the stream. */
+ksvd_status ksvd_profile_counters(ksvd_ctx* ctx, int64_t* out, int count);
+
+/* ---- config.json (batch_denoiser.cpp:36-118) ------------------------------
+ * The reference's keys: inputFolder, outputFolder, files[] {name, ref, and
+ * per-file overrides}, globalParams {patchWidthDim, patchHeightDim,
+ * slidingWidth, slidingHeight, atoms, ksvdIter, ompIter, B&W, speckle, type,
+ * minOmpIterBatch, subImageWidthDim, subImageHeightDim}; additional optional
+ * keys noiseVariance, precision ("FP32" | "BF16" | "FP16") and compat. */
+
+/* Number of files in a config.json, -1 if it cannot be read. */
+int ksvd_batch_count(const char* json_path);
+/* Parameters and paths of file `index` (output name <out>/<pw>_<ph>_<name>
+ * as in batch_denoiser.cpp:96).  Strings are truncated to cap bytes; a
+ * noise variance <= 0 means "estimate from the image". */
+ksvd_status ksvd_batch_entry(const char* json_path, int index, ksvd_params* p, char* input_path,
+                             char* output_path, char* ref_path, size_t cap, double* noise_variance);
+/* testBatchDenoiser (src/main.cpp:56-112): denoises every file of the config
+ * (PGM/PPM in, 8-bit PGM out) and, if verbose, prints the per-image report.
+ * Returns the number of failed images, -1 for an unreadable config. */
+int ksvd_run_batch(const char* json_path, int verbose);
 
 #ifdef __cplusplus
 }

@@ -75,7 +75,7 @@ def support_agreement(i1, i2):
     return float(np.mean(np.all(i1 == i2, axis=1)))
 
 
-@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("precision", [0, 1, 2])
 @pytest.mark.parametrize("K,L", [(64, 5), (32, 3), (256, 5), (100, 8)])
 def test_omp_vs_fp64_oracle(torch_cuda, ksvd, oracle, case, K, L, precision):
     _, noisy = case
@@ -91,7 +91,7 @@ def test_omp_vs_fp64_oracle(torch_cuda, ksvd, oracle, case, K, L, precision):
     assert rel.max() < 1e-4, rel.max()
 
 
-@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("precision", [0, 1, 2])
 def test_omp_img512_patches(torch_cuda, ksvd, oracle, synth, precision):
     """12x12 patches of the 512^2 workload image (27,889 patches, 144-dim),
     256 atoms, L = 5: support agreement with the FP64 oracle >= 99.9%."""
@@ -109,7 +109,7 @@ def test_omp_img512_patches(torch_cuda, ksvd, oracle, synth, precision):
     assert rel.max() < 1e-4, rel.max()
 
 
-@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("precision", [0, 1, 2])
 def test_omp_edge_cases(torch_cuda, ksvd, oracle, precision):
     # zero patches, exactly representable patches, fewer patches than a tile
     r = np.random.default_rng(5)
@@ -222,7 +222,7 @@ def test_codes_to_dense(torch_cuda, ksvd, oracle, case, geo):
     np.testing.assert_array_equal(dense.cpu().numpy(), ref)
 
 
-@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("precision", [0, 1, 2])
 @pytest.mark.parametrize("compat,q1", [(1, False), (3, True)])
 def test_denoise_psnr_vs_fp64_oracle(torch_cuda, ksvd, oracle, synth, compat, q1, precision):
     clean = synth.clean_image(128, 31)
@@ -282,7 +282,7 @@ def test_zero_image_reports_zero_atom(torch_cuda, ksvd):
 
 
 @pytest.mark.slow
-@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("precision", [0, 1, 2])
 def test_denoise_img512_workload_vs_fp64_oracle(torch_cuda, ksvd, oracle, synth, precision):
     """The 512^2 workload (sigma 20, 12x12 stride 3, 256 atoms, L=5, 10
     iterations), reference-compatible mode, against the FP64 oracle."""
