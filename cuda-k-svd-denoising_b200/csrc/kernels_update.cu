@@ -195,8 +195,10 @@ struct UpdLayout {
 
 __host__ __device__ inline size_t upd_al16(size_t x) { return (x + 15) & ~size_t(15); }
 
-// Two residual-column buffers, three record buffers, two gathered-coefficient
-// buffers, the mbarriers (3 for records, 2 for columns).
+// Three residual-column buffers (the third lets the next atom's first chunk
+// be fetched while the current atom still uses its buffers), three record
+// buffers, one gathered-coefficient buffer per column buffer, the mbarriers
+// (3 for records, 3 for columns).
 __host__ __device__ inline UpdLayout upd_layout(int n, int K, int L, bool dsmem) {
   const int npad = (n + 15) / 16 * 16;
   const int R = (L + 2 + 3) / 4 * 4;
@@ -205,11 +207,11 @@ __host__ __device__ inline UpdLayout upd_layout(int n, int K, int L, bool dsmem)
   o.off_ds = off;
   off = upd_al16(off + (dsmem ? size_t(K) * n * 4 : 0));
   o.off_e = off;
-  off = upd_al16(off + size_t(2) * kEChunk * n * 4);
+  off = upd_al16(off + size_t(3) * kEChunk * n * 4);
   o.off_rec = off;
   off = upd_al16(off + size_t(3) * kEChunk * R * 4);
   o.off_cf = off;
-  off = upd_al16(off + size_t(2) * kEChunk * L * 4);
+  off = upd_al16(off + size_t(3) * kEChunk * L * 4);
   o.off_u = off;
   off = upd_al16(off + size_t(npad) * 4);
   o.off_dold = off;
@@ -217,7 +219,7 @@ __host__ __device__ inline UpdLayout upd_layout(int n, int K, int L, bool dsmem)
   o.off_red = off;
   off = upd_al16(off + 64 * 4);
   o.off_bar = off;
-  off = upd_al16(off + 5 * 8);
+  off = upd_al16(off + 6 * 8);
   o.total = off;
   return o;
 }
@@ -247,7 +249,7 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
   float* u = reinterpret_cast<float*>(usm + lo.off_u);
   float* dold = reinterpret_cast<float*>(usm + lo.off_dold);
   float* red = reinterpret_cast<float*>(usm + lo.off_red);
-  unsigned long long* bars = reinterpret_cast<unsigned long long*>(usm + lo.off_bar);  // [0..2] rec, [3..4] col
+  unsigned long long* bars = reinterpret_cast<unsigned long long*>(usm + lo.off_bar);  // [0..2] rec, [3..5] col
   (void)N;
 
   const unsigned G = gridDim.x;
@@ -259,7 +261,7 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
   float* my_escr = escr + size_t(b) * size_t(escr_cap) * n;
 
   if (tid == 0) {
-    for (int k = 0; k < 5; ++k) mbar_init(&bars[k], 1);
+    for (int k = 0; k < 6; ++k) mbar_init(&bars[k], 1);
     fence_mbar_init();
   }
   if (DSMEM)
@@ -385,13 +387,36 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
     }
   };
 
+  // Column buffers of the k-th processed atom: chunk 0 in buffer P = k & 1
+  // (fetched ahead during the previous atom), later chunks alternate between
+  // buffer 2 and buffer 1 - P; the coefficient pass streams through P and 2,
+  // so buffer 1 - P is free for the next atom's first chunk.
+  int kproc = 0;
+  bool prefetched = false;  // records of chunks 0/1 and patches of chunk 0 in flight
   for (int j = 0; j < K; ++j) {
     const int beg = atom_ptr[j];
     const int c = atom_ptr[j + 1] - beg;
     if (c == 0) continue;
+    const int P = kproc & 1;
+    ++kproc;
+    auto colbuf = [&](int ch) { return ch == 0 ? P : ((ch & 1) ? 2 : 1 - P); };
     const int c_eff = (q1_cap && c > 1024) ? 1024 : c;
     const int active = min(int(G), (c_eff + kMinEntriesPerCta - 1) / kMinEntriesPerCta);
     for (int i = tid; i < npad; i += kUpdThreads) dold[i] = (i < n) ? datom(j, i) : 0.0f;
+    // the next atom with a non-empty support and this CTA's first chunk of it
+    int jn = j + 1;
+    while (jn < K && atom_ptr[jn + 1] == atom_ptr[jn]) ++jn;
+    int nbeg = 0, nsb = 0, nse = 0;
+    bool n_in = false;
+    if (jn < K) {
+      nbeg = atom_ptr[jn];
+      const int cn = atom_ptr[jn + 1] - nbeg;
+      const int cne = (q1_cap && cn > 1024) ? 1024 : cn;
+      const int nact = min(int(G), (cne + kMinEntriesPerCta - 1) / kMinEntriesPerCta);
+      nsb = int(int64_t(cne) * b / nact);
+      nse = int(int64_t(cne) * (b + 1) / nact);
+      n_in = b < nact;
+    }
 
     // ---- phase A: partial Gram of this CTA's residual columns -------------
     const int sb = int(int64_t(c_eff) * b / active), se = int(int64_t(c_eff) * (b + 1) / active);
@@ -405,19 +430,22 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
         for (int s2 = 0; s2 < TN; ++s2) blk[r][s2] = 0.0f;
       lap(0);
       float cfv[kCfRegs];
-      issue_records(beg, sb, min(kEChunk, se - sb), 0);
-      if (nch > 1) issue_records(beg, sb + kEChunk, min(kEChunk, se - sb - kEChunk), 1);
-      if (!records_ready(0)) return;
-      issue_patches(min(kEChunk, se - sb), 0, 0, true);
+      if (!prefetched) {
+        issue_records(beg, sb, min(kEChunk, se - sb), 0);
+        if (nch > 1) issue_records(beg, sb + kEChunk, min(kEChunk, se - sb - kEChunk), 1);
+        if (!records_ready(0)) return;
+        issue_patches(min(kEChunk, se - sb), 0, colbuf(0), true);
+      }
+      // coefficients change with every atom: gathered only now
       gather_load(min(kEChunk, se - sb), 0, cfv);
-      gather_store(min(kEChunk, se - sb), 0, cfv);
+      gather_store(min(kEChunk, se - sb), colbuf(0), cfv);
       lap(11);
       for (int ch = 0; ch < nch; ++ch) {
-        const int buf = ch & 1, r3 = ch % 3;
+        const int buf = colbuf(ch), r3 = ch % 3;
         const int t0 = sb + ch * kEChunk;
         const int m = min(kEChunk, se - t0);
         const int m1 = min(kEChunk, se - t0 - kEChunk);  // next chunk (if any)
-        if (ch + 1 < nch) issue_patches(m1, (ch + 1) % 3, buf ^ 1, false);
+        if (ch + 1 < nch) issue_patches(m1, (ch + 1) % 3, colbuf(ch + 1), false);
         if (ch + 2 < nch) issue_records(beg, t0 + 2 * kEChunk, min(kEChunk, se - t0 - 2 * kEChunk), (ch + 2) % 3);
         lap(11);
         if (!finish(m, r3, buf, !resident && tma, t0 - sb)) return;
@@ -444,7 +472,7 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
 #pragma unroll
             for (int s2 = 0; s2 < TN; ++s2) blk[r][s2] = fmaf(ra[r], rb[s2], blk[r][s2]);
         }
-        if (ch + 1 < nch) gather_store(m1, buf ^ 1, cfv);
+        if (ch + 1 < nch) gather_store(m1, colbuf(ch + 1), cfv);
         fence_proxy_async_smem();
         __syncthreads();
         lap(13);
@@ -459,11 +487,19 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
         }
     }
     __syncthreads();
+    // records of the next atom's first chunks (immutable during the sweep)
+    prefetched = false;
+    if (n_in && tma) {
+      issue_records(nbeg, nsb, min(kEChunk, nse - nsb), 0);
+      if (nse - nsb > kEChunk) issue_records(nbeg, nsb + kEChunk, min(kEChunk, nse - nsb - kEChunk), 1);
+      prefetched = true;
+    }
     lap(0);
     if (!grid_sync(bar, G)) return;
     lap(1);
 
     // ---- phase B: fixed-order sum of the active partial Grams --------------
+    if (prefetched) issue_patches(min(kEChunk, nse - nsb), 0, 1 - P, false);
     {
       const int qb = int(int64_t(nn) * b / G), qe = int(int64_t(nn) * (b + 1) / G);
       for (int q = qb + tid; q < qe; q += kUpdThreads) {
@@ -564,7 +600,7 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
         }
       };
       if (resident) {
-        dots(0, sb, se - sb);  // buffer 0 still holds this CTA's columns
+        dots(P, sb, se - sb);  // buffer P still holds this CTA's columns
         fence_proxy_async_smem();
       } else if (!tma) {
         // rows not 16-byte aligned: rebuild the columns (generic loads)
@@ -585,9 +621,10 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
       } else {
         // stream the columns back from the scratch
         if (tid == 0) bulk_wait0();  // this CTA's scratch stores are complete
+        auto sbuf = [&](int ch) { return (ch & 1) ? 2 : P; };
         auto issue_cols = [&](int ch) {
           if (tid == 0 && !failed) {
-            const int t0 = sb + ch * kEChunk, m = min(kEChunk, se - t0), buf = ch & 1;
+            const int t0 = sb + ch * kEChunk, m = min(kEChunk, se - t0), buf = sbuf(ch);
             mbar_arrive_expect_tx(&bars[3 + buf], unsigned(m) * unsigned(n) * 4u);
             bulk_g2s(Ebase + size_t(buf) * kEChunk * n, my_escr + size_t(t0 - sb) * n, unsigned(m) * unsigned(n) * 4u,
                      &bars[3 + buf]);
@@ -596,7 +633,7 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
         __syncthreads();  // the scratch is complete before it is read back
         issue_cols(0);
         for (int ch = 0; ch < nch; ++ch) {
-          const int buf = ch & 1;
+          const int buf = sbuf(ch);
           const int t0 = sb + ch * kEChunk;
           const int m = min(kEChunk, se - t0);
           if (ch + 1 < nch) issue_cols(ch + 1);
