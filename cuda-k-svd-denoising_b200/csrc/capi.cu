@@ -219,6 +219,7 @@ const char* ksvd_status_string(int st) {
     case KSVD_ERR_TIMEOUT: return "device wait timed out";
     case KSVD_ERR_NUMERIC: return "numerical failure";
     case KSVD_ERR_NO_DEVICE: return "no CUDA device";
+    case KSVD_ERR_TOO_LARGE: return "size beyond the fixed maximum";
     default: return "unknown status";
   }
 }

@@ -22,6 +22,7 @@ CUDA_K_GESVD, CUDA_K_GESVDJ, CUDA_K_GESVDA, CUDA_K_SM100A = 0, 1, 2, 3
 # ksvd_status
 OK, ERR_LOAD, ERR_DENOISE, ERR_SAVE = 0, -1, -2, -3
 ERR_INVALID, ERR_CUDA, ERR_NO_MEMORY, ERR_TIMEOUT, ERR_NUMERIC, ERR_NO_DEVICE = -10, -11, -12, -13, -14, -15
+ERR_TOO_LARGE = -16
 # ksvd_precision
 PREC_FP32, PREC_BF16_RESCORE, PREC_FP16_RESCORE = 0, 1, 2
 # compat flags
@@ -151,6 +152,8 @@ def lib():
         L.ksvd_batch_entry.restype = _int
         L.ksvd_run_batch.argtypes = [ctypes.c_char_p, _int]
         L.ksvd_run_batch.restype = _int
+        L.ksvd_omp_noalloc.argtypes = [P, _vp, _i64, _vp, _vp, _vp, _vp]
+        L.ksvd_omp_noalloc.restype = _int
         _lib = L
     return _lib
 
@@ -311,6 +314,13 @@ class Context:
 
     def launch_count(self) -> int:
         return int(lib().ksvd_launch_count(self.h))
+
+
+def omp_noalloc(params: KsvdParams, patches, dictionary, idx, coef, stream_handle: int | None = None) -> int:
+    """ksvd_omp_noalloc: OMP without a context or any device allocation
+    (torch CUDA tensors on the current device).  Returns the status."""
+    return int(lib().ksvd_omp_noalloc(ctypes.byref(params), _ptr(patches), patches.shape[0], _ptr(dictionary),
+                                      _ptr(idx), _ptr(coef), stream_handle))
 
 
 def batch_config(path: str) -> list[dict]:

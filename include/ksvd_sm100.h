@@ -61,7 +61,8 @@ typedef enum ksvd_status {
   KSVD_ERR_NO_MEMORY = -12,
   KSVD_ERR_TIMEOUT = -13, /* a bounded device wait gave up                     */
   KSVD_ERR_NUMERIC = -14, /* zero-norm initial atom or non-finite data         */
-  KSVD_ERR_NO_DEVICE = -15
+  KSVD_ERR_NO_DEVICE = -15,
+  KSVD_ERR_TOO_LARGE = -16 /* beyond the fixed maximum of ksvd_omp_noalloc      */
 } ksvd_status;
 
 /* Arithmetic of the OMP correlation D^T R.  The tensor-core forms re-score
@@ -217,6 +218,24 @@ ksvd_status ksvd_profile_phases(ksvd_ctx* ctx, double* ms_out, int count);
  * updated, [2] tensor-core OMP error windows wider than its candidate list,
  * [3] tensor-core OMP exact re-scores.  Synchronises the stream. */
 ksvd_status ksvd_profile_counters(ksvd_ctx* ctx, int64_t* out, int count);
+
+/* OMP sparse coding (the same FP32 kernels and results as ksvd_omp) for
+ * callers that cannot allocate device memory: code inside a CUDA graph being
+ * captured or replayed, plugins whose host framework owns every device
+ * allocation, real-time loops that must not allocate once running.  It needs
+ * no context and allocates nothing: the caller passes p (patch size, atoms,
+ * omp_iter are used), the patches (num_patches x n), the dictionary (atoms x
+ * n) and the outputs idx / coef (num_patches x omp_iter), all on the current
+ * device, and the stream (NULL = legacy default stream).  The dictionary Gram
+ * lives in a 2 MiB array compiled into the library, so atoms is limited to
+ * 512 (KSVD_ERR_TOO_LARGE beyond).  Every call on a device shares that array:
+ * calls whose work overlaps on the GPU (e.g. on two streams) race; serialise
+ * them.  The first call on each device looks the array's address up and
+ * caches it; make it before starting any stream capture.
+ * It has no counterpart in the reference (whose OMP allocates on every call,
+ * cublas_matrix_omp.cu:79,125-165,254-255). */
+ksvd_status ksvd_omp_noalloc(const ksvd_params* p, const float* d_patches, int64_t num_patches,
+                             const float* d_dict, int32_t* d_idx, float* d_coef, void* stream);
 
 /* ---- config.json (batch_denoiser.cpp:36-118) ------------------------------
  * The reference's keys: inputFolder, outputFolder, files[] {name, ref, and
