@@ -119,31 +119,45 @@ def dist_env():
     return rank, world, local
 
 
-def cpu_baseline(pkg, oracle, wl, budget_s=20.0, max_patches=None):
-    """One K-SVD iteration (OMP + update) of the CPU FP32 restatement on a
-    bounded contiguous sample of the workload's patches, all host threads."""
+def _cpu_sample_size(oracle, Y, D, wl, budget_s):
+    """Patches per timed CPU iteration: the whole workload when one iteration
+    is estimated to fit the budget, else a contiguous middle slice sized for it.
+    The estimate separates the per-patch cost (OMP, Gram build) from the
+    per-atom cost of the update (one n x n eigenproblem per atom)."""
+    N = Y.shape[0]
+    n1, n2 = min(N, 2048), min(N, 8192)
+    times = []
+    for ns in (n1, n2):
+        Ys = np.ascontiguousarray(Y[(N - ns) // 2:(N - ns) // 2 + ns])
+        t = time.perf_counter()
+        idx, coef = oracle.omp(Ys, D, wl.omp_iter, dtype=np.float32)
+        oracle.update_dictionary(Ys, D, idx, coef, q1_cap=False, dtype=np.float32)
+        times.append(time.perf_counter() - t)
+    per_patch = max((times[1] - times[0]) / max(n2 - n1, 1), 1e-9)
+    fixed = max(times[0] - per_patch * n1, 0.0)
+    if fixed + per_patch * N <= budget_s:
+        return N
+    return int(min(N, max(n2, (budget_s - fixed) / per_patch)))
+
+
+def cpu_baseline(pkg, oracle, wl, budget_s=40.0):
+    """One K-SVD iteration (FP32 OMP + full update sweep) of the CPU
+    restatement, all host threads, on the whole workload if it fits the budget."""
     clean, noisy = wl.images()
     Y = oracle.extract_patches(noisy, wl.patch, wl.patch, wl.stride, wl.stride)
     N = Y.shape[0]
     D = oracle.init_dictionary(Y, wl.atoms, int_norm=True, dtype=np.float32)
-    # calibrate on a small slice, then size the sample for the budget
-    n0 = min(N, 4096)
-    t = time.perf_counter()
-    idx, coef = oracle.omp(Y[:n0], D, wl.omp_iter, dtype=np.float32)
-    oracle.update_dictionary(Y[:n0], D, idx, coef, q1_cap=False, dtype=np.float32)
-    dt = time.perf_counter() - t
-    ns = int(min(N, max(n0, n0 * budget_s / max(dt, 1e-3) * 0.8)))
-    if max_patches:
-        ns = min(ns, max_patches)
+    ns = _cpu_sample_size(oracle, Y, D, wl, budget_s)
     start = (N - ns) // 2
     Ys = np.ascontiguousarray(Y[start:start + ns])
     t = time.perf_counter()
     idx, coef = oracle.omp(Ys, D, wl.omp_iter, dtype=np.float32)
     oracle.update_dictionary(Ys, D, idx, coef, q1_cap=False, dtype=np.float32)
     dt = time.perf_counter() - t
+    what = "all" if ns == N else f"a contiguous middle slice of {ns}"
     return {"value": ns / dt, "unit": "patches/s", "cores": oracle.max_threads(), "kind": "port",
-            "sample": f"1 K-SVD iteration (FP32 OMP + full update sweep) on {ns} of the workload's {N} patches "
-                      f"(contiguous middle slice), {wl.atoms} atoms, L={wl.omp_iter}, {dt:.1f} s"}, dt
+            "sample": f"1 K-SVD iteration (FP32 OMP + full update sweep, {wl.atoms} atoms, L={wl.omp_iter}) on "
+                      f"{what} of the workload's {N} patches, {dt:.1f} s"}, dt
 
 
 def run_reference(args, wl):
@@ -156,14 +170,9 @@ def run_reference(args, wl):
     Y = oracle.extract_patches(noisy, wl.patch, wl.patch, wl.stride, wl.stride)
     N = Y.shape[0]
     D0 = oracle.init_dictionary(Y, wl.atoms, int_norm=True, dtype=np.float32)
-    # size each step so that warmup + steps fit in about two minutes
-    n0 = min(N, 4096)
-    t = time.perf_counter()
-    idx, coef = oracle.omp(Y[:n0], D0, wl.omp_iter, dtype=np.float32)
-    oracle.update_dictionary(Y[:n0], D0, idx, coef, q1_cap=False, dtype=np.float32)
-    per_patch = (time.perf_counter() - t) / n0
+    # each step sized so that warmup + steps fit in about three minutes
     steps_total = args.steps + args.warmup
-    ns = int(min(N, max(n0, 120.0 / steps_total / max(per_patch, 1e-9))))
+    ns = _cpu_sample_size(oracle, Y, D0, wl, 180.0 / steps_total)
     start = (N - ns) // 2
     Ys = np.ascontiguousarray(Y[start:start + ns])
     D = D0.copy()
@@ -185,8 +194,8 @@ def run_reference(args, wl):
                    "patch": f"{wl.patch}x{wl.patch}", "stride": wl.stride, "num_patches": N, "atoms": wl.atoms,
                    "omp_iter": wl.omp_iter, "sample_patches": ns},
         "cpu_baseline": {"value": value, "unit": "patches/s", "cores": cores, "kind": "port",
-                         "sample": f"each step: 1 K-SVD iteration on {ns} of {N} patches (contiguous middle "
-                                   f"slice), FP32 CPU restatement, {cores} threads"},
+                         "sample": f"each step: 1 K-SVD iteration of the FP32 CPU restatement on "
+                                   f"{'all' if ns == N else ns} of the workload's {N} patches, {cores} threads"},
         "e2e": {"value": value, "unit": "patches/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -200,11 +209,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="img2048_p12s3_k256")
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16", "fp16"])
+    ap.add_argument("--precision", default="fp16", choices=["fp32", "bf16", "fp16"],
+                    help="headline form; the other forms are timed beside it unless --no-forms")
+    ap.add_argument("--no-forms", action="store_true")
     ap.add_argument("--compat", type=int, default=1, help="KSVD_COMPAT_* bits (1 = INT_NORM, 3 = +Q1 cap)")
     ap.add_argument("--e2e-calls", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--cpu-budget", type=float, default=40.0)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -223,13 +234,18 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
 
     ksvd = pkg.ksvd
-    prec = {"fp32": ksvd.PREC_FP32, "bf16": ksvd.PREC_BF16_RESCORE, "fp16": ksvd.PREC_FP16_RESCORE}[args.precision]
-    params = ksvd.make_params(patch_width_dim=wl.patch, patch_height_dim=wl.patch, sliding_width=wl.stride,
-                              sliding_height=wl.stride, atoms=wl.atoms, omp_iter=wl.omp_iter,
-                              ksvd_iter=wl.ksvd_iter, precision=prec, compat=args.compat, device=local)
-    ctx = ksvd.Context(params)
+    precs = {"fp32": ksvd.PREC_FP32, "bf16": ksvd.PREC_BF16_RESCORE, "fp16": ksvd.PREC_FP16_RESCORE}
+
+    def make_ctx(form):
+        params = ksvd.make_params(patch_width_dim=wl.patch, patch_height_dim=wl.patch, sliding_width=wl.stride,
+                                  sliding_height=wl.stride, atoms=wl.atoms, omp_iter=wl.omp_iter,
+                                  ksvd_iter=wl.ksvd_iter, precision=precs[form], compat=args.compat, device=local)
+        c = ksvd.Context(params)
+        c.set_stream(stream.cuda_stream)
+        return c, params
+
     stream = torch.cuda.Stream()
-    ctx.set_stream(stream.cuda_stream)
+    ctx, params = make_ctx(args.precision)
 
     # each rank: its own seeded image (replicas)
     from dataclasses import replace
@@ -252,46 +268,66 @@ def main():
     D0 = D.clone()
     stream.synchronize()
 
-    # ---- warm-up, then K timed K-SVD iterations ---------------------------
-    for _ in range(args.warmup):
-        ctx.iterate(patches, D, idx, coef, 1)
-    stream.synchronize()
-    with torch.cuda.stream(stream):
-        D.copy_(D0)
-    ctx.profile(True)
-    ctx.profile_reset()
-    launches0 = ctx.launch_count()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clocks:
+    def timed_steps(c, sample_clocks):
+        """W warm-up iterations, then K timed ones from the initial dictionary.
+        Returns (ms per step max over ranks, per-family ms, phases, counters,
+        launches, clock summary)."""
+        with torch.cuda.stream(stream):
+            D.copy_(D0)
+        for _ in range(args.warmup):
+            c.iterate(patches, D, idx, coef, 1)
+        stream.synchronize()
+        with torch.cuda.stream(stream):
+            D.copy_(D0)
+        c.profile(True)
+        c.profile_reset()
+        l0 = c.launch_count()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        sampler = ClockSampler(local) if sample_clocks else None
+        if sampler:
+            sampler.__enter__()
         ev0.record(stream)
         for _ in range(args.steps):
-            ctx.iterate(patches, D, idx, coef, 1)
+            c.iterate(patches, D, idx, coef, 1)
         ev1.record(stream)
         torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    ms_total = ev0.elapsed_time(ev1)
-    gpu_launches = ctx.launch_count() - launches0
-    fam = {f: ctx.profile_read(f) for f in ("gram", "omp", "csr", "update")}
-    phases = ctx.profile_phases()
-    counters = ctx.profile_counters()
-    ctx.profile(False)
-    ms_step = ms_total / args.steps
-    if dist:
-        t = torch.tensor([ms_step], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_step = float(t.item())
+        if sampler:
+            sampler.__exit__(None, None, None)
+        if dist:
+            dist.barrier()
+        ms = ev0.elapsed_time(ev1) / args.steps
+        fams = {f: c.profile_read(f) for f in ("gram", "omp", "csr", "update")}
+        ph = c.profile_phases()
+        cn = c.profile_counters()
+        c.profile(False)
+        if dist:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, fams, ph, cn, c.launch_count() - l0, (sampler.summary() if sampler else None)
+
+    # ---- the headline form: warm-up, then K timed K-SVD iterations ---------
+    ms_step, fam, phases, counters, gpu_launches, clk_summary = timed_steps(ctx, True)
     value = N * world / (ms_step / 1000.0)
+    forms = {args.precision: value}
+    if not args.no_forms:
+        for form in ("fp32", "fp16", "bf16"):
+            if form == args.precision:
+                continue
+            c2, _ = make_ctx(form)
+            ms2 = timed_steps(c2, False)[0]
+            forms[form] = N * world / (ms2 / 1000.0)
+            c2.close()
 
     # ---- e2e through the C ABI with pinned host buffers --------------------
     img_h = torch.from_numpy(noisy).pin_memory()
     out_h = torch.empty_like(img_h).pin_memory()
     e2e_ms = []
     st = None
-    for i in range(args.e2e_calls + 1):
+    for i in range(max(args.e2e_calls, 1) + 1):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         st = ctx.denoise_ptr(img_h.data_ptr(), W, H, sigma2, out_h.data_ptr())
@@ -339,7 +375,7 @@ def main():
             "metric": "patches/s per K-SVD iteration", "value": value, "unit": "patches/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": {"fp32": "f32", "bf16": "bf16+f32", "fp16": "f16+f32"}[args.precision],
+            "dtype": {"fp32": "f32", "bf16": "bf16+f32+f64", "fp16": "f16+f32+f64"}[args.precision],
             "data": "synthetic",
             "config": {"workload": wl.name, "image": f"{wl.size}x{wl.size}", "sigma": wl.sigma,
                        "patch": f"{wl.patch}x{wl.patch}", "stride": wl.stride, "num_patches": N, "atoms": K,
@@ -362,7 +398,8 @@ def main():
             "counters_per_step": {k: v / max(args.steps, 1) for k, v in counters.items()},
             "quality": {"psnr_noisy": psnr_noisy, "psnr_denoised": psnr_out,
                         "power_iters_last_sweep": st.power_iters, "atoms_updated_last_sweep": st.atoms_updated},
-            "clocks": clocks.summary(),
+            "forms_patches_per_s": forms,
+            "clocks": clk_summary,
         }
         if cpu:
             line["cpu_baseline"] = cpu

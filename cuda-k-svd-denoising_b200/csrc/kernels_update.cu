@@ -663,6 +663,8 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
 __global__ void accumulate_phases_kernel(const DevStats* __restrict__ src, DevStats* __restrict__ dst) {
   const int t = threadIdx.x;
   if (t < 16) dst->phase_ns[t] += src->phase_ns[t];
+  if (t == 16) dst->power_iters += src->power_iters;
+  if (t == 17) dst->atoms_updated += src->atoms_updated;
 }
 
 cudaError_t launch_accumulate_phases(const DevStats* src, DevStats* dst, cudaStream_t s) {

@@ -5,6 +5,12 @@
 // path, by bench.py as the timed CPU baseline ("port"), and nowhere else:
 // the product library never links or calls it.
 //
+// Parity unpinned: the reference ships no golden vectors for this path and
+// its own GPU code could not be run to make some (its denoiser layer needs
+// the absent CImg library; its OMP layer aborted with an illegal address on
+// a B200).  The restatement is checked against independent numpy / LAPACK
+// restatements of each step instead.
+//
 // Every function names the reference lines it follows.  The scalar type T is
 // double for the FP64 oracle and float for the FP32 restatement; the tiny
 // dense solves (Cholesky of the support Gram, the n x n eigenproblem) are

@@ -192,3 +192,13 @@ def ksvd_denoise(noisy: np.ndarray, sigma2: float, *, pw=8, ph=8, sw=2, sh=2, at
 
 if os.environ.get("KSVD_ORACLE_THREADS"):
     set_threads(int(os.environ["KSVD_ORACLE_THREADS"]))
+
+
+def compact_to_dense(idx: np.ndarray, coef: np.ndarray, K: int) -> np.ndarray:
+    """Compact codes (N, L) -> dense (N, K); unused slots (idx < 0) skipped."""
+    N, L = idx.shape
+    out = np.zeros((N, K), dtype=np.float64)
+    rows = np.repeat(np.arange(N), L)
+    m = idx.reshape(-1) >= 0
+    out[rows[m], idx.reshape(-1)[m]] = coef.reshape(-1)[m]
+    return out
