@@ -299,7 +299,7 @@ def main():
         if dist:
             dist.barrier()
         ms = ev0.elapsed_time(ev1) / args.steps
-        fams = {f: c.profile_read(f) for f in ("gram", "omp", "csr", "update")}
+        fams = {f: c.profile_read(f) for f in ("gram", "omp", "csr", "residual", "update")}
         ph = c.profile_phases()
         cn = c.profile_counters()
         c.profile(False)
@@ -392,9 +392,9 @@ def main():
             "kernel_ms_per_step": {f: fam[f][0] / max(args.steps, 1) for f in fam},
             "phase_ms_per_step": {
                 name: phases[i] / max(args.steps, 1) for i, name in (
-                    (0, "upd_gram"), (1, "upd_wait1"), (2, "upd_sum"), (3, "upd_wait2"), (4, "upd_power"),
-                    (5, "upd_coef"), (6, "upd_wait3"), (8, "omp_corr"), (9, "omp_ls"), (10, "omp_io"),
-                    (11, "upd_gram_stage"), (12, "upd_gram_finish"), (13, "upd_gram_acc"), (14, "upd_gload"))},
+                    (7, "upd_setup"), (0, "upd_wait_prev_atom"), (1, "upd_load"), (2, "upd_pass"),
+                    (3, "upd_wait_partials"), (4, "upd_allreduce"), (5, "upd_coef_store"), (8, "omp_corr"),
+                    (9, "omp_ls"), (10, "omp_io"))},
             "counters_per_step": {k: v / max(args.steps, 1) for k, v in counters.items()},
             "quality": {"psnr_noisy": psnr_noisy, "psnr_denoised": psnr_out,
                         "power_iters_last_sweep": st.power_iters, "atoms_updated_last_sweep": st.atoms_updated},

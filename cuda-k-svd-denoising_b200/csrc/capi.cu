@@ -158,7 +158,8 @@ ksvd_status check_kernel_support(ksvd_ctx* c) {
     if (!ksvd::omp_tc_supported(n, c->p.atoms, c->p.omp_iter))
       return fail(c, KSVD_ERR_INVALID, "patch size x atoms too large for the tensor-core OMP kernel");
   }
-  if (!ksvd::update_supported(n)) return fail(c, KSVD_ERR_INVALID, "patch size > 160 not supported by the update kernel");
+  if (!ksvd::update_res_supported(n))
+    return fail(c, KSVD_ERR_INVALID, "patch size > 512 not supported by the update kernel");
   return KSVD_OK;
 }
 
@@ -435,24 +436,29 @@ static ksvd_status update_impl(ksvd_ctx* c, const float* d_patches, int64_t N, f
   KSVD_TRY(wsT(c, "csr_counts", size_t(w.nchunks) * K, &w.chunk_counts));
   KSVD_TRY(wsT(c, "csr_atom_ptr", size_t(2) * K + 1, &w.atom_ptr));
   KSVD_TRY(wsT(c, "csr_entries", size_t(N) * L, &w.entries));
-  KSVD_TRY(wsT(c, "csr_records", size_t(N) * L * ksvd::csr_record_ints(L), &w.records));
-  const int grid = ksvd::update_grid_size(n, K, L, c->num_sms);
+  w.records = nullptr;  // the residual-based sweep needs only the entries
+  const int grid = ksvd::update_res_grid_size(n, c->num_sms);
   if (grid < 1) return fail(c, KSVD_ERR_CUDA, "update kernel cannot be made co-resident");
-  float *gpart = nullptr, *gsum = nullptr, *escr = nullptr;
-  KSVD_TRY(wsT(c, "upd_gpart", size_t(grid) * n * n, &gpart));
-  KSVD_TRY(wsT(c, "upd_gsum", size_t(n) * n, &gsum));
-  const int64_t escr_cap = ksvd::update_scratch_cap(N, grid);
-  KSVD_TRY(wsT(c, "upd_escr", size_t(grid) * size_t(escr_cap) * n, &escr));
+  float *resid = nullptr, *gw = nullptr;
+  unsigned* sync = nullptr;
+  KSVD_TRY(wsT(c, "upd_resid", size_t(N) * n, &resid));
+  KSVD_TRY(wsT(c, "upd_partials", ksvd::update_res_partial_floats(n, grid), &gw));
+  KSVD_TRY(wsT(c, "upd_sync", size_t(2) * K, &sync));
   {
     Prof pr(c, "csr", 4);
     KSVD_CU(c, ksvd::launch_csr_build(d_idx, d_coef, N, L, K, w, c->stream), "csr build");
   }
+  {
+    Prof pr(c, "residual", 1);
+    KSVD_CU(c, ksvd::launch_residual(d_patches, N, n, d_dict, K, L, d_idx, d_coef, resid, c->num_sms, c->stream),
+            "residual");
+  }
   KSVD_CU(c, cudaMemsetAsync(c->d_stats, 0, sizeof(ksvd::DevStats), c->stream), "stats reset");
   Prof pr(c, "update", 1);
   KSVD_CU(c,
-          ksvd::launch_update(d_patches, N, n, d_dict, K, L, d_idx, d_coef, w,
-                              (c->p.compat & KSVD_COMPAT_Q1_CAP) ? 1 : 0, gpart, gsum, escr, escr_cap, c->d_flags,
-                              c->d_stats, grid, c->stream),
+          ksvd::launch_update_res(resid, n, d_dict, K, L, d_coef, w.atom_ptr, w.entries,
+                                  (c->p.compat & KSVD_COMPAT_Q1_CAP) ? 1 : 0, gw, sync, c->d_flags, c->d_stats, grid,
+                                  c->stream),
           "update");
   if (c->profiling) {
     // fold this sweep's phase timers into the profiling accumulator

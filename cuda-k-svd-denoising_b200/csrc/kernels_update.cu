@@ -139,6 +139,7 @@ __global__ void __launch_bounds__(kCsrChunk) csr_fill_kernel(const int32_t* __re
       for (int s2 = 0; s2 < L; ++s2) rank += (wa[l2 * L + s2] == a);
     const int pos = wcnt[warp * K + a] + rank;
     entries[pos] = int(p * L + s);
+    if (!records) continue;
     const int R = (L + 2 + 3) / 4 * 4;
     int* rec = records + int64_t(pos) * R;
     rec[0] = int(p);

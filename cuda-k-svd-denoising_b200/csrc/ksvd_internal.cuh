@@ -37,9 +37,11 @@ struct DevStats {
   unsigned long long omp_rescore_misses;  // tensor-core OMP: error windows wider than the candidate list
   unsigned long long pad;                 // tensor-core OMP: exact re-scores
   // Wall time (ns) CTA 0 spends in each phase of the persistent kernels:
-  // update: [0] gram build, [1] wait after it, [2] partial sum, [3] wait,
-  // [4] power iteration, [5] coefficients, [6] wait; omp: [8] correlation +
-  // argmax, [9] least squares + residual, [10] tile load/store.
+  // update: [7] slice set-up, [0] wait for the previous atom, [1] column
+  // load, [2] local power pass, [3] wait for the other CTAs' partials,
+  // [4] partial all-reduce + normalisation, [5] coefficients + residual;
+  // omp: [8] correlation + argmax, [9] least squares + residual, [10] tile
+  // load/store.
   unsigned long long phase_ns[16];
 };
 
@@ -102,6 +104,17 @@ cudaError_t launch_update(const float* patches, int64_t N, int n, float* dict, i
                           const int32_t* idx, float* coef, CsrWork w, int q1_cap, float* gpart,
                           float* gsum, float* escr, int64_t escr_cap, GridBarrier* bar, DevStats* stats,
                           int grid, cudaStream_t s);
+
+// Dictionary update on a maintained residual (kernels_update_res.cu).
+bool update_res_supported(int n);
+int update_res_grid_size(int n, int num_sms);
+size_t update_res_partial_floats(int n, int grid);
+cudaError_t launch_residual(const float* Y, int64_t N, int n, const float* D, int K, int L, const int32_t* idx,
+                            const float* coef, float* R, int num_sms, cudaStream_t s);
+// sync: 2K unsigned words (zeroed by the launch); gw: update_res_partial_floats.
+cudaError_t launch_update_res(float* R, int n, float* D, int K, int L, float* coef, const int* atom_ptr,
+                              const int* entries, int q1_cap, float* gw, unsigned* sync, GridBarrier* flags,
+                              DevStats* stats, int grid, cudaStream_t s);
 
 // Image rebuild.
 cudaError_t launch_col2im(const float* noisy, const PatchGeom& g, const float* dict, int K, int L,
