@@ -279,7 +279,7 @@ def main():
         stream.synchronize()
         with torch.cuda.stream(stream):
             D.copy_(D0)
-        c.profile(True)
+        c.profile(1)
         c.profile_reset()
         l0 = c.launch_count()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -300,9 +300,14 @@ def main():
             dist.barrier()
         ms = ev0.elapsed_time(ev1) / args.steps
         fams = {f: c.profile_read(f) for f in ("gram", "omp", "csr", "residual", "update")}
-        ph = c.profile_phases()
         cn = c.profile_counters()
-        c.profile(False)
+        # one more (untimed) iteration with the in-kernel phase timers on
+        c.profile_reset()
+        c.profile(2)
+        c.iterate(patches, D, idx, coef, 1)
+        ph = c.profile_phases()
+        cn.update({k: v for k, v in c.profile_counters().items() if k.startswith("omp_")})
+        c.profile(0)
         if dist:
             t = torch.tensor([ms], device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -390,12 +395,13 @@ def main():
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
                          "algorithmic_bytes_per_patch": bytes_per_patch, "avg_launch_ms": avg_ms},
             "kernel_ms_per_step": {f: fam[f][0] / max(args.steps, 1) for f in fam},
-            "phase_ms_per_step": {
-                name: phases[i] / max(args.steps, 1) for i, name in (
+            "phase_ms_one_step": {
+                name: phases[i] for i, name in (
                     (7, "upd_setup"), (0, "upd_wait_prev_atom"), (1, "upd_load"), (2, "upd_pass"),
                     (3, "upd_wait_partials"), (4, "upd_allreduce"), (5, "upd_coef_store"), (8, "omp_corr"),
-                    (9, "omp_ls"), (10, "omp_io"))},
-            "counters_per_step": {k: v / max(args.steps, 1) for k, v in counters.items()},
+                    (9, "omp_ls"), (10, "omp_io"), (11, "omp_rescore"))},
+            "counters_per_step": {k: (v if k.startswith("omp_") else v / max(args.steps, 1))
+                                  for k, v in counters.items()},
             "quality": {"psnr_noisy": psnr_noisy, "psnr_denoised": psnr_out,
                         "power_iters_last_sweep": st.power_iters, "atoms_updated_last_sweep": st.atoms_updated},
             "forms_patches_per_s": forms,

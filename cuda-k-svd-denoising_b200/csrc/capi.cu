@@ -296,7 +296,7 @@ void* ksvd_get_stream(const ksvd_ctx* c) { return c ? static_cast<void*>(c->stre
 
 ksvd_status ksvd_profile_enable(ksvd_ctx* c, int enable) {
   if (!c) return KSVD_ERR_INVALID;
-  c->profiling = enable != 0;
+  c->profiling = enable < 0 ? 0 : (enable > 2 ? 2 : enable);
   return KSVD_OK;
 }
 
@@ -407,12 +407,12 @@ static ksvd_status omp_impl(ksvd_ctx* c, const float* d_patches, int64_t N, cons
     KSVD_CU(c,
             ksvd::launch_omp_tc(d_patches, N, n, d_dict, gram, K, L, d_idx, d_coef, c->num_sms,
                                 c->p.precision == KSVD_PREC_FP16_RESCORE ? 1 : 0, c->d_flags,
-                                c->profiling ? c->d_phase : nullptr, c->stream),
+                                c->profiling >= 2 ? c->d_phase : nullptr, c->stream),
             "omp (tensor cores)");
   } else {
     KSVD_CU(c,
             ksvd::launch_omp_fp32(d_patches, N, n, d_dict, gram, K, L, d_idx, d_coef, c->num_sms,
-                                  c->profiling ? c->d_phase : nullptr, c->stream),
+                                  c->profiling >= 2 ? c->d_phase : nullptr, c->stream),
             "omp");
   }
   return KSVD_OK;
@@ -457,8 +457,8 @@ static ksvd_status update_impl(ksvd_ctx* c, const float* d_patches, int64_t N, f
   Prof pr(c, "update", 1);
   KSVD_CU(c,
           ksvd::launch_update_res(resid, n, d_dict, K, L, d_coef, w.atom_ptr, w.entries,
-                                  (c->p.compat & KSVD_COMPAT_Q1_CAP) ? 1 : 0, gw, sync, c->d_flags, c->d_stats, grid,
-                                  c->stream),
+                                  (c->p.compat & KSVD_COMPAT_Q1_CAP) ? 1 : 0, gw, sync, c->d_flags, c->d_stats,
+                                  c->profiling >= 2 ? 1 : 0, grid, c->stream),
           "update");
   if (c->profiling) {
     // fold this sweep's phase timers into the profiling accumulator

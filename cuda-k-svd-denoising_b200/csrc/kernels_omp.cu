@@ -124,11 +124,15 @@ __global__ void __launch_bounds__(kOmpThreads, 1)
 
   const int ag = tid >> 3, pg = tid & 7;  // atom group (32), patch group (8)
   const bool timer = (blockIdx.x == 0 && tid == 0 && stats != nullptr);
+  // phase times (slots 8..11) gather in shared memory, flushed once at the end
+  __shared__ unsigned long long s_ph[4];
+  if (timer)
+    for (int k = 0; k < 4; ++k) s_ph[k] = 0ull;
   unsigned long long tmark = timer ? globaltimer_ns() : 0ull;
   auto lap = [&](int slot) {
     if (timer) {
       const unsigned long long t = globaltimer_ns();
-      stats->phase_ns[slot] += t - tmark;
+      s_ph[slot - 8] += t - tmark;
       tmark = t;
     }
   };
@@ -334,6 +338,8 @@ __global__ void __launch_bounds__(kOmpThreads, 1)
     __syncthreads();
     lap(10);
   }
+  if (timer)
+    for (int k = 0; k < 4; ++k) atomicAdd(&stats->phase_ns[8 + k], s_ph[k]);
 }
 
 size_t omp_fp32_smem_bytes(int n, int K, int L) { return omp_layout(n, K, L).total; }

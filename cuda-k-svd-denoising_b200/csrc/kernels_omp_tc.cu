@@ -286,11 +286,15 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   auto Lat = [&](int i, int j) -> double& { return Lp[i * (i + 1) / 2 + j]; };
 
   const bool timer = (blockIdx.x == 0 && tid == 0 && stats != nullptr);
+  // phase times (slots 8..11) gather in shared memory, flushed once at the end
+  __shared__ unsigned long long s_ph[4];
+  if (timer)
+    for (int k = 0; k < 4; ++k) s_ph[k] = 0ull;
   unsigned long long tmark = timer ? globaltimer_ns() : 0ull;
   auto lap = [&](int slot) {
     if (timer) {
       const unsigned long long t = globaltimer_ns();
-      stats->phase_ns[slot] += t - tmark;
+      s_ph[slot - 8] += t - tmark;
       tmark = t;
     }
   };
@@ -591,6 +595,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     __syncthreads();
   }
   if (stats && nscored) atomicAdd(&stats->pad, (unsigned long long)nscored);
+  if (timer)
+    for (int k = 0; k < 4; ++k) atomicAdd(&stats->phase_ns[8 + k], s_ph[k]);
   // ---- teardown --------------------------------------------------------------
   if (failed && tid == 0) mbar_wait(mbar, phase, kMmaWaitNs);  // bounded drain of MMAs in flight
   tc_fence_before();

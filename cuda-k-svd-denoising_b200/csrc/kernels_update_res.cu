@@ -105,7 +105,7 @@ template <int NW>
 __global__ void __launch_bounds__(kUrThreads, 1)
     update_res_kernel(float* R, int n, float* D, int K, int L, float* coef, const int* __restrict__ atom_ptr,
                       const int* __restrict__ entries, int q1_cap, int cap, float* gw, unsigned* sync,
-                      GridBarrier* flags, DevStats* stats) {
+                      GridBarrier* flags, DevStats* stats, int timers) {
   extern __shared__ __align__(16) unsigned char ursm[];
   const int n4 = ur_n4(n);
   float* Es = reinterpret_cast<float*>(ursm);
@@ -116,6 +116,7 @@ __global__ void __launch_bounds__(kUrThreads, 1)
   float* wred = dold + n4;
   float* red = wred + kUrWarps * n4;
   __shared__ int s_ok;
+  __shared__ unsigned long long s_ph[8];  // phase times of this CTA (slots 0..7)
 
   const int G = int(gridDim.x), b = int(blockIdx.x);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -126,12 +127,15 @@ __global__ void __launch_bounds__(kUrThreads, 1)
   if (Gr > kUrWarps) Gr = kUrWarps;
   if (Gr < 1) Gr = 1;
 
-  const bool timer = (b == 0 && tid == 0);
+  // phase times gather in shared memory and are flushed once at the end
+  const bool timer = (timers != 0 && b == 0 && tid == 0);
+  if (timer)
+    for (int k = 0; k < 8; ++k) s_ph[k] = 0ull;
   unsigned long long tmark = timer ? globaltimer_ns() : 0ull;
   auto lap = [&](int slot) {
     if (timer) {
       const unsigned long long t = globaltimer_ns();
-      stats->phase_ns[slot] += t - tmark;
+      s_ph[slot] += t - tmark;
       tmark = t;
     }
   };
@@ -342,6 +346,8 @@ __global__ void __launch_bounds__(kUrThreads, 1)
     }
     lap(5);
   }
+  if (timer)
+    for (int k = 0; k < 8; ++k) atomicAdd(&stats->phase_ns[k], s_ph[k]);
 }
 
 template <int NW>
@@ -397,7 +403,7 @@ cudaError_t launch_residual(const float* Y, int64_t N, int n, const float* D, in
 
 cudaError_t launch_update_res(float* R, int n, float* D, int K, int L, float* coef, const int* atom_ptr,
                               const int* entries, int q1_cap, float* gw, unsigned* sync, GridBarrier* flags,
-                              DevStats* stats, int grid, cudaStream_t s) {
+                              DevStats* stats, int timers, int grid, cudaStream_t s) {
   void* fn = pick_update_res(n);
   const int cap = update_res_capacity(n);
   if (!fn || cap < 16 || grid < 1) return cudaErrorInvalidValue;
@@ -409,7 +415,7 @@ cudaError_t launch_update_res(float* R, int n, float* D, int K, int L, float* co
   int capv = cap;
   void* args[] = {(void*)&R,       (void*)&n,       (void*)&D,      (void*)&K,    (void*)&L,
                   (void*)&coef,    (void*)&atom_ptr, (void*)&entries, (void*)&q1_cap, (void*)&capv,
-                  (void*)&gw,      (void*)&sync,    (void*)&flags,  (void*)&stats};
+                  (void*)&gw,      (void*)&sync,    (void*)&flags,  (void*)&stats,   (void*)&timers};
   return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kUrThreads), args, smem, s);
 }
 

@@ -41,7 +41,7 @@ struct DevStats {
   // load, [2] local power pass, [3] wait for the other CTAs' partials,
   // [4] partial all-reduce + normalisation, [5] coefficients + residual;
   // omp: [8] correlation + argmax, [9] least squares + residual, [10] tile
-  // load/store.
+  // load/store, [11] exact re-scores.
   unsigned long long phase_ns[16];
 };
 
@@ -86,7 +86,8 @@ struct CsrWork {
   int* chunk_counts;   // nchunks x K
   int* atom_ptr;       // 2K + 1 (atom_ptr[0..K], then scratch)
   int* entries;        // N * L (patch * L + slot), grouped by atom, ascending patch
-  int* records;        // N * L records of csr_record_ints(L) ints, same order:
+  int* records;        // optional (nullptr: not written): N * L records of
+                       // csr_record_ints(L) ints, same order:
                        // {patch, slot, atom of slot 0..L-1 (-1 if unused), pad}
   int64_t nchunks;
 };
@@ -94,16 +95,7 @@ inline int csr_record_ints(int L) { return (L + 2 + 3) / 4 * 4; }
 int64_t csr_num_chunks(int64_t N);
 cudaError_t launch_csr_build(const int32_t* idx, const float* coef, int64_t N, int L, int K, CsrWork w,
                              cudaStream_t s);
-bool update_supported(int n);
 cudaError_t launch_accumulate_phases(const DevStats* src, DevStats* dst, cudaStream_t s);
-size_t update_smem_bytes(int n, int K, int L);
-int update_grid_size(int n, int K, int L, int num_sms);
-// Residual-column scratch: grid x cap x n floats, cap = update_scratch_cap(N, grid).
-int64_t update_scratch_cap(int64_t N, int grid);
-cudaError_t launch_update(const float* patches, int64_t N, int n, float* dict, int K, int L,
-                          const int32_t* idx, float* coef, CsrWork w, int q1_cap, float* gpart,
-                          float* gsum, float* escr, int64_t escr_cap, GridBarrier* bar, DevStats* stats,
-                          int grid, cudaStream_t s);
 
 // Dictionary update on a maintained residual (kernels_update_res.cu).
 bool update_res_supported(int n);
@@ -112,9 +104,10 @@ size_t update_res_partial_floats(int n, int grid);
 cudaError_t launch_residual(const float* Y, int64_t N, int n, const float* D, int K, int L, const int32_t* idx,
                             const float* coef, float* R, int num_sms, cudaStream_t s);
 // sync: 2K unsigned words (zeroed by the launch); gw: update_res_partial_floats.
+// stats receives the counters always, the phase times when timers != 0.
 cudaError_t launch_update_res(float* R, int n, float* D, int K, int L, float* coef, const int* atom_ptr,
                               const int* entries, int q1_cap, float* gw, unsigned* sync, GridBarrier* flags,
-                              DevStats* stats, int grid, cudaStream_t s);
+                              DevStats* stats, int timers, int grid, cudaStream_t s);
 
 // Image rebuild.
 cudaError_t launch_col2im(const float* noisy, const PatchGeom& g, const float* dict, int K, int L,
@@ -151,7 +144,7 @@ struct ksvd_ctx {
     double total_ms = 0.0;
     int64_t launches = 0;
   };
-  bool profiling = false;
+  int profiling = 0;  // 0 off, 1 per-family event timing, 2 + in-kernel phase timers
   std::map<std::string, Family> families;
   std::vector<cudaEvent_t> event_pool;
   int64_t launch_count = 0;

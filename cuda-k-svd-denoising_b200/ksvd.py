@@ -289,8 +289,9 @@ class Context:
         return st
 
     # -- profiling --------------------------------------------------------
-    def profile(self, enable: bool = True):
-        self._check(lib().ksvd_profile_enable(self.h, int(enable)))
+    def profile(self, level: int = 1):
+        """0 off, 1 per-family event timing, 2 + in-kernel phase timers."""
+        self._check(lib().ksvd_profile_enable(self.h, int(level)))
 
     def profile_reset(self):
         self._check(lib().ksvd_profile_reset(self.h))

@@ -198,8 +198,10 @@ ksvd_status ksvd_build_image(ksvd_ctx* ctx, const float* d_noisy, int width, int
 ksvd_status ksvd_codes_to_dense(ksvd_ctx* ctx, const int32_t* d_idx, const float* d_coef,
                                 int64_t num_patches, float* d_dense);
 
-/* Per-kernel device timing: when enabled, every kernel family records CUDA
- * events around its launches on the context's stream. */
+/* Profiling level.  1: every kernel family records CUDA events around its
+ * launches on the context's stream, and the update's counters accumulate.
+ * 2: in addition the persistent kernels time their phases on the device and
+ * the tensor-core OMP counts its exact re-scores (slightly slower).  0: off. */
 ksvd_status ksvd_profile_enable(ksvd_ctx* ctx, int enable);
 /* Sum of launch durations (ms) and launch count of a kernel family since the
  * last reset ("im2col", "init_dict", "gram", "omp", "csr", "update", "col2im",
@@ -209,14 +211,17 @@ ksvd_status ksvd_profile_reset(ksvd_ctx* ctx);
 /* Total number of kernels this context launched since creation. */
 int64_t ksvd_launch_count(const ksvd_ctx* ctx);
 /* Wall time (ms) the first CTA of the persistent kernels spent per phase
- * while profiling was enabled (since the last reset): [0] update Gram build,
- * [1] grid wait, [2] partial-Gram sum, [3] grid wait, [4] power iteration,
- * [5] coefficients, [6] grid wait, [8] OMP correlation + argmax, [9] OMP least
- * squares + residual, [10] OMP tile load/store.  Synchronises the stream. */
+ * while profiling at level 2 (since the last reset): update [7] slice set-up,
+ * [0] wait for the previous atom, [1] column load, [2] local power pass,
+ * [3] wait for the other CTAs' partials, [4] partial all-reduce and
+ * normalisation, [5] coefficients and residual store; OMP [8] correlation +
+ * argmax, [9] least squares + residual, [10] tile load/store, [11] exact
+ * re-scores.  Synchronises the stream. */
 ksvd_status ksvd_profile_phases(ksvd_ctx* ctx, double* ms_out, int count);
 /* Counters accumulated while profiling: [0] power iterations, [1] atoms
- * updated, [2] tensor-core OMP error windows wider than its candidate list,
- * [3] tensor-core OMP exact re-scores.  Synchronises the stream. */
+ * updated (level >= 1), [2] tensor-core OMP error windows wider than its
+ * candidate list, [3] tensor-core OMP exact re-scores (level 2).
+ * Synchronises the stream. */
 ksvd_status ksvd_profile_counters(ksvd_ctx* ctx, int64_t* out, int count);
 
 /* OMP sparse coding (the same FP32 kernels and results as ksvd_omp) for
