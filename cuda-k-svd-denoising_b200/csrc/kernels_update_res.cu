@@ -35,29 +35,35 @@ namespace ksvd {
 
 constexpr int kUrThreads = 512;
 constexpr int kUrWarps = kUrThreads / 32;
-constexpr int kUrTargetSlice = 96;    // entries per CTA before another CTA joins an atom
+constexpr int kUrTargetSlice = 64;    // entries per CTA before another CTA joins an atom
 constexpr int kUrMaxIters = 200;
 constexpr float kUrTol = 2.0e-7f;     // max |u_new - u_old| to stop
 constexpr size_t kUrSmemMax = 232448 - 256;  // opt-in shared memory per block, less the static part
 
 __host__ __device__ inline int ur_n4(int n) { return (n + 3) & ~3; }
 
-// Shared memory: [cap x n4] columns | ent[2][cap] | xold[2][cap] | u[n4] |
-// dold[n4] | dnext[n4] | wred[kUrWarps x n4]
+// Row stride of the resident columns (floats): a multiple of 4 whose float4
+// count is odd, so that the 8 rows a quarter-warp reads with 16-byte loads
+// sit in distinct banks.
+__host__ __device__ inline int ur_es(int n) { return 4 * ((ur_n4(n) / 4) | 1); }
+constexpr int kUrRows = 32;  // reduction rows: 16 column groups + 16 streaming warps
+
+// Shared memory: [cap x es] columns | ent[2][cap] | xold[2][cap] | u[n4] |
+// dold[n4] | dnext[n4] | wred[kUrRows x n4]
 __host__ __device__ inline size_t ur_fixed_bytes(int n) {
   const int n4 = ur_n4(n);
-  return size_t(n4) * 4 * 3 + size_t(kUrWarps) * n4 * 4;
+  return size_t(n4) * 4 * 3 + size_t(kUrRows) * n4 * 4;
 }
 
 int update_res_capacity(int n) {
-  const size_t per = size_t(ur_n4(n)) * 4 + 16;
+  const size_t per = size_t(ur_es(n)) * 4 + 16;
   const size_t fixed = ur_fixed_bytes(n);
   if (fixed + per * 16 > kUrSmemMax) return 0;
   // a multiple of 4 keeps u, dold, dnext and wred (read as float4) 16-byte aligned
   return int((kUrSmemMax - fixed) / per) & ~3;
 }
 
-size_t update_res_smem_bytes(int n, int cap) { return size_t(cap) * (size_t(ur_n4(n)) * 4 + 16) + ur_fixed_bytes(n); }
+size_t update_res_smem_bytes(int n, int cap) { return size_t(cap) * (size_t(ur_es(n)) * 4 + 16) + ur_fixed_bytes(n); }
 
 // Bounded spin of thread 0 until *ctr >= target.  False on timeout or when an
 // error is already flagged.
@@ -113,26 +119,39 @@ __global__ void __launch_bounds__(kUrThreads, 1)
                       const int* __restrict__ entries, int q1_cap, int cap, float* gw, unsigned* sync,
                       GridBarrier* flags, DevStats* stats, int timers) {
   extern __shared__ __align__(16) unsigned char ursm[];
-  const int n4 = ur_n4(n);
+  const int n4 = ur_n4(n), es = ur_es(n);
+  const int F = n4 / 4, es4 = es / 4;  // float4 per row of u / w, per resident column
   float* Es = reinterpret_cast<float*>(ursm);
-  int* ent_b = reinterpret_cast<int*>(ursm + size_t(cap) * n4 * 4);  // [2][cap]
+  const float4* Es4 = reinterpret_cast<const float4*>(ursm);
+  int* ent_b = reinterpret_cast<int*>(ursm + size_t(cap) * es * 4);  // [2][cap]
   float* xold_b = reinterpret_cast<float*>(ent_b + 2 * cap);           // [2][cap]
   float* u = xold_b + 2 * cap;
   float* dold = u + n4;
   float* dnext = dold + n4;
-  float* wred = dnext + n4;
+  float* wred = dnext + n4;  // [kUrRows][n4]
+  float4* u4 = reinterpret_cast<float4*>(u);
+  const float4* dold4 = reinterpret_cast<const float4*>(dold);
+  float4* wred4 = reinterpret_cast<float4*>(wred);
   __shared__ int s_ok;
   __shared__ int s_stop;
+  __shared__ __align__(8) unsigned long long s_mbar;  // completion of the residual-row bulk copies
   __shared__ unsigned long long s_ph[8];  // phase times of this CTA (slots 0..7)
 
   const int G = int(gridDim.x), b = int(blockIdx.x);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   unsigned* iter_cnt = sync;
   unsigned* done_cnt = sync + K;
-  const int F = n4 / 4;                       // float4 per partial row
-  int Gr = kUrThreads / F;                    // reduction groups
-  if (Gr > kUrWarps) Gr = kUrWarps;
+  int Gr = kUrThreads / F;  // column groups of the w pass, partial groups of the all-reduce
+  if (Gr > 16) Gr = 16;
   if (Gr < 1) Gr = 1;
+  // bulk copies need 16-byte aligned rows of a multiple of 16 bytes
+  const bool tma = (n & 3) == 0 && (reinterpret_cast<uintptr_t>(R) & 15) == 0;
+  unsigned mpar = 0;  // parity of the next phase of s_mbar
+  if (tid == 0) {
+    mbar_init(&s_mbar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
 
   // phase times gather in shared memory and are flushed once at the end
   const bool timer = (timers != 0 && b == 0 && tid == 0);
@@ -189,6 +208,20 @@ __global__ void __launch_bounds__(kUrThreads, 1)
     }
     for (int i = tid; i < n4; i += kUrThreads) dst[i] = (i < n) ? __ldcg(D + int64_t(a) * n + i) : 0.0f;
   };
+  // u . e_q for a resident column (one thread, 16-byte loads, 4 chains)
+  auto dot_u = [&](int q) -> float {
+    const float4* er = Es4 + size_t(q) * es4;
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+#pragma unroll 6
+    for (int f = 0; f < F; ++f) {
+      const float4 e = er[f], w = u4[f];
+      a0 = fmaf(e.x, w.x, a0);
+      a1 = fmaf(e.y, w.y, a1);
+      a2 = fmaf(e.z, w.z, a2);
+      a3 = fmaf(e.w, w.w, a3);
+    }
+    return (a0 + a1) + (a2 + a3);
+  };
 
   int jprev = -1, aprev = 0;
   int slot = 0;        // meta buffer of the current atom
@@ -207,8 +240,11 @@ __global__ void __launch_bounds__(kUrThreads, 1)
     // columns [0, mc) of the slice enter the power iteration
     int mc = c_eff - sb;
     mc = mc < 0 ? 0 : (mc > m ? m : mc);
+    const int mcr = mc < cap ? mc : cap;  // of which resident
+    const bool streamed = mc > cap;        // some enter from the residual
     const int* ent_s = ent_b + slot * cap;
     const float* xold_s = xold_b + slot * cap;
+    float* v_s = xold_b + slot * cap;  // per-column scalars once the columns are built
 
     // ---- entries, old coefficients and the old atom: never written by other
     // atoms, so read before the wait (or prefetched during the previous atom)
@@ -233,42 +269,40 @@ __global__ void __launch_bounds__(kUrThreads, 1)
       prefetch = b < nact;
     }
 
-    // ---- resident columns e_q = r_q + x_q d_old (loads batched) -----------
-    if ((n & 3) == 0) {
-      constexpr int kB = 8;
-      const int total = mres * F;
-      for (int f0 = tid; f0 < total; f0 += kUrThreads * kB) {
-        float4 r[kB];
-#pragma unroll
-        for (int k = 0; k < kB; ++k) {
-          const int f = f0 + k * kUrThreads;
-          if (f < total) {
-            const int q = f / F, i4 = f - q * F;
-            r[k] = __ldcg(reinterpret_cast<const float4*>(R + int64_t(ent_s[q] / L) * n) + i4);
-          }
-        }
-#pragma unroll
-        for (int k = 0; k < kB; ++k) {
-          const int f = f0 + k * kUrThreads;
-          if (f < total) {
-            const int q = f / F, i4 = f - q * F;
-            const float x = xold_s[q];
-            const float4 d = reinterpret_cast<const float4*>(dold)[i4];
-            float4 e;
-            e.x = fmaf(x, d.x, r[k].x);
-            e.y = fmaf(x, d.y, r[k].y);
-            e.z = fmaf(x, d.z, r[k].z);
-            e.w = fmaf(x, d.w, r[k].w);
-            reinterpret_cast<float4*>(Es + size_t(q) * n4)[i4] = e;
-          }
-        }
+    // ---- resident columns e_q = r_q + x_q d_old ---------------------------
+    if (tma) {
+      // residual rows by bulk copies (the residual was written by other CTAs
+      // through the generic proxy: acquire above, proxy fence here), then
+      // e = r + x d in place
+      if (tid == 0) mbar_arrive_expect_tx(&s_mbar, unsigned(mres) * unsigned(n) * 4u);
+      __syncthreads();
+      asm volatile("fence.proxy.async.global;" ::: "memory");
+      for (int q = tid; q < mres; q += kUrThreads)
+        bulk_g2s(Es + size_t(q) * es, R + int64_t(ent_s[q] / L) * n, unsigned(n) * 4u, &s_mbar);
+      const bool ok = mbar_wait(&s_mbar, mpar, kBarrierTimeoutNs);
+      mpar ^= 1u;
+      if (__syncthreads_or(!ok)) {
+        if (tid == 0) atomicCAS(&flags->err, DEVERR_NONE, DEVERR_TIMEOUT);
+        return;
+      }
+      for (int t = tid; t < mres * F; t += kUrThreads) {
+        const int q = t / F, f = t - q * F;
+        const float x = xold_s[q];
+        const float4 d = dold4[f];
+        float4* ep = reinterpret_cast<float4*>(Es) + size_t(q) * es4 + f;
+        float4 e = *ep;
+        e.x = fmaf(x, d.x, e.x);
+        e.y = fmaf(x, d.y, e.y);
+        e.z = fmaf(x, d.z, e.z);
+        e.w = fmaf(x, d.w, e.w);
+        *ep = e;
       }
     } else {
-      for (int f = tid; f < mres * n4; f += kUrThreads) {
-        const int q = f / n4, i = f - q * n4;
+      for (int t = tid; t < mres * n4; t += kUrThreads) {
+        const int q = t / n4, i = t - q * n4;
         float e = 0.0f;
         if (i < n) e = fmaf(xold_s[q], dold[i], __ldcg(R + int64_t(ent_s[q] / L) * n + i));
-        Es[size_t(q) * n4 + i] = e;
+        Es[size_t(q) * es + i] = e;
       }
     }
     for (int i = tid; i < n4; i += kUrThreads) u[i] = dold[i];
@@ -296,59 +330,81 @@ __global__ void __launch_bounds__(kUrThreads, 1)
     // ---- power iteration ---------------------------------------------------
     int iters = 0;
     float dprev = 0.0f;  // warp 0: the previous step's change
-    const int mcr = mc < cap ? mc : cap;
     for (int it = 0; it < kUrMaxIters; ++it) {
-      float ur[NW], wacc[NW];
-#pragma unroll
-      for (int k = 0; k < NW; ++k) {
-        const int i = lane + 32 * k;
-        ur[k] = (i < n) ? u[i] : 0.0f;
-        wacc[k] = 0.0f;
-      }
-      for (int q = warp; q < mcr; q += kUrWarps) {  // resident columns
-        const float* er = Es + size_t(q) * n4;
-        float ev[NW];
-        float dp = 0.0f;
+      // v_q = u . e_q, one thread per resident column
+      for (int q = tid; q < mcr; q += kUrThreads) v_s[q] = dot_u(q);
+      if (streamed) {  // columns beyond the capacity: a warp per two columns
+        float ur[NW], wacc[NW];
 #pragma unroll
         for (int k = 0; k < NW; ++k) {
           const int i = lane + 32 * k;
-          ev[k] = (i < n) ? er[i] : 0.0f;
-          dp = fmaf(ur[k], ev[k], dp);
+          ur[k] = (i < n) ? u[i] : 0.0f;
+          wacc[k] = 0.0f;
         }
-        dp = warp_sum(dp);
+        for (int q = cap + warp; q < mc; q += 2 * kUrWarps) {
+          float e0[NW], e1[NW];
+          int ea, eb;
+          stream_cols(q, mc, e0, e1, ea, eb);
+          float d0 = 0.0f, d1 = 0.0f;
 #pragma unroll
-        for (int k = 0; k < NW; ++k) wacc[k] = fmaf(dp, ev[k], wacc[k]);
-      }
-      for (int q = cap + warp; q < mc; q += 2 * kUrWarps) {  // streamed columns
-        float e0[NW], e1[NW];
-        int ea, eb;
-        stream_cols(q, mc, e0, e1, ea, eb);
-        float d0 = 0.0f, d1 = 0.0f;
+          for (int k = 0; k < NW; ++k) {
+            d0 = fmaf(ur[k], e0[k], d0);
+            d1 = fmaf(ur[k], e1[k], d1);
+          }
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) {
+            d0 += __shfl_xor_sync(0xffffffffu, d0, o);
+            d1 += __shfl_xor_sync(0xffffffffu, d1, o);
+          }
+#pragma unroll
+          for (int k = 0; k < NW; ++k) wacc[k] = fmaf(d1, e1[k], fmaf(d0, e0[k], wacc[k]));
+        }
 #pragma unroll
         for (int k = 0; k < NW; ++k) {
-          d0 = fmaf(ur[k], e0[k], d0);
-          d1 = fmaf(ur[k], e1[k], d1);
+          const int i = lane + 32 * k;
+          if (i < n4) wred[(16 + warp) * n4 + i] = wacc[k];
         }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          d0 += __shfl_xor_sync(0xffffffffu, d0, o);
-          d1 += __shfl_xor_sync(0xffffffffu, d1, o);
-        }
-#pragma unroll
-        for (int k = 0; k < NW; ++k) wacc[k] = fmaf(d1, e1[k], fmaf(d0, e0[k], wacc[k]));
-      }
-#pragma unroll
-      for (int k = 0; k < NW; ++k) {
-        const int i = lane + 32 * k;
-        if (i < n4) wred[warp * n4 + i] = wacc[k];
       }
       __syncthreads();
-      float* gwp = gw + (size_t(it & 1) * G + b) * n4;
-      for (int i = tid; i < n4; i += kUrThreads) {
-        float s = 0.0f;
+      // w = sum_q v_q e_q: column group g (q = g mod Gr) of float4 column f
+      {
+        const int f = tid % F, g = tid / F;
+        if (g < Gr) {
+          float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll 4
+          for (int q = g; q < mcr; q += Gr) {
+            const float v = v_s[q];
+            const float4 e = Es4[size_t(q) * es4 + f];
+            acc.x = fmaf(v, e.x, acc.x);
+            acc.y = fmaf(v, e.y, acc.y);
+            acc.z = fmaf(v, e.z, acc.z);
+            acc.w = fmaf(v, e.w, acc.w);
+          }
+          wred4[g * F + f] = acc;
+        }
+      }
+      __syncthreads();
+      float4* gwp = reinterpret_cast<float4*>(gw + (size_t(it & 1) * G + b) * n4);
+      for (int f = tid; f < F; f += kUrThreads) {
+        float4 acc = wred4[f];
+#pragma unroll 4
+        for (int g = 1; g < Gr; ++g) {
+          const float4 v = wred4[g * F + f];
+          acc.x += v.x;
+          acc.y += v.y;
+          acc.z += v.z;
+          acc.w += v.w;
+        }
+        if (streamed)
 #pragma unroll
-        for (int w = 0; w < kUrWarps; ++w) s += wred[w * n4 + i];
-        __stcg(gwp + i, s);
+          for (int w = 0; w < kUrWarps; ++w) {
+            const float4 v = wred4[(16 + w) * F + f];
+            acc.x += v.x;
+            acc.y += v.y;
+            acc.z += v.z;
+            acc.w += v.w;
+          }
+        __stcg(gwp + f, acc);
       }
       __syncthreads();
       lap(2);
@@ -380,7 +436,7 @@ __global__ void __launch_bounds__(kUrThreads, 1)
               acc.w += v[k].w;
             }
           }
-          reinterpret_cast<float4*>(wred + g * n4)[f] = acc;
+          wred4[g * F + f] = acc;
         }
       }
       __syncthreads();
@@ -388,16 +444,24 @@ __global__ void __launch_bounds__(kUrThreads, 1)
       // warp 0 finishes the step: w, its norm, the new u, the change, the
       // stop decision and, when stopping, the sign (u . d_old >= 0)
       if (warp == 0) {
-        float wv[NW];
+        constexpr int kF = 4;  // float4 per lane (F <= 128)
+        float4 wv[kF];
         float s2 = 0.0f;
 #pragma unroll
-        for (int k = 0; k < NW; ++k) {
-          const int i = lane + 32 * k;
-          float wi = 0.0f;
-          if (i < n)
-            for (int g = 0; g < Gr; ++g) wi += wred[g * n4 + i];
-          wv[k] = wi;
-          s2 = fmaf(wi, wi, s2);
+        for (int k = 0; k < kF; ++k) {
+          const int f = lane + 32 * k;
+          float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (f < F)
+#pragma unroll 4
+            for (int g = 0; g < Gr; ++g) {
+              const float4 v = wred4[g * F + f];
+              acc.x += v.x;
+              acc.y += v.y;
+              acc.z += v.z;
+              acc.w += v.w;
+            }
+          wv[k] = acc;
+          s2 = fmaf(acc.x, acc.x, fmaf(acc.y, acc.y, fmaf(acc.z, acc.z, fmaf(acc.w, acc.w, s2))));
         }
         const float nrm2 = warp_sum(s2);
         bool stop;
@@ -407,35 +471,51 @@ __global__ void __launch_bounds__(kUrThreads, 1)
           const float inv = 1.0f / sqrtf(nrm2);
           float dm = 0.0f;
 #pragma unroll
-          for (int k = 0; k < NW; ++k) {
-            const int i = lane + 32 * k;
-            if (i < n) {
-              const float un = wv[k] * inv;
-              dm = fmaxf(dm, fabsf(un - u[i]));
-              u[i] = un;
+          for (int k = 0; k < kF; ++k) {
+            const int f = lane + 32 * k;
+            if (f < F) {
+              const float4 o = u4[f];
+              float4 un;
+              un.x = wv[k].x * inv;
+              un.y = wv[k].y * inv;
+              un.z = wv[k].z * inv;
+              un.w = wv[k].w * inv;
+              dm = fmaxf(dm, fmaxf(fmaxf(fabsf(un.x - o.x), fabsf(un.y - o.y)),
+                                   fmaxf(fabsf(un.z - o.z), fabsf(un.w - o.w))));
+              u4[f] = un;
             }
           }
           dm = warp_max(dm);
-          // stop when the change is below the tolerance, or when the
-          // observed contraction rho = dm / dprev puts the remaining distance
-          // to the limit, about dm * rho / (1 - rho), below it
+          // stop when the change is below the tolerance, or when the observed
+          // contraction rho = dm / dprev puts the remaining distance to the
+          // limit, about dm rho / (1 - rho), below it
           const float rho = (it > 0 && dprev > 0.0f) ? dm / dprev : 1.0f;
-          stop = dm < kUrTol || (rho < 0.5f && dm < 1e-3f && dm * rho < 0.5f * kUrTol * (1.0f - rho) * 2.0f);
+          stop = dm < kUrTol || (rho < 0.5f && dm < 1e-3f && dm * rho < kUrTol * (1.0f - rho));
           dprev = dm;
         }
         if (stop) {
           float sd = 0.0f;
 #pragma unroll
-          for (int k = 0; k < NW; ++k) {
-            const int i = lane + 32 * k;
-            if (i < n) sd = fmaf(u[i], dold[i], sd);
+          for (int k = 0; k < kF; ++k) {
+            const int f = lane + 32 * k;
+            if (f < F) {
+              const float4 a = u4[f], d = dold4[f];
+              sd = fmaf(a.x, d.x, fmaf(a.y, d.y, fmaf(a.z, d.z, fmaf(a.w, d.w, sd))));
+            }
           }
           sd = warp_sum(sd);
           if (sd < 0.0f)
 #pragma unroll
-            for (int k = 0; k < NW; ++k) {
-              const int i = lane + 32 * k;
-              if (i < n) u[i] = -u[i];
+            for (int k = 0; k < kF; ++k) {
+              const int f = lane + 32 * k;
+              if (f < F) {
+                float4 a = u4[f];
+                a.x = -a.x;
+                a.y = -a.y;
+                a.z = -a.z;
+                a.w = -a.w;
+                u4[f] = a;
+              }
             }
         }
         if (lane == 0) s_stop = stop ? 1 : 0;
@@ -453,35 +533,19 @@ __global__ void __launch_bounds__(kUrThreads, 1)
     }
 
     // ---- coefficients x = u . e (0 beyond the cap) and residual e - x u ----
-    {
+    for (int q = tid; q < mres; q += kUrThreads) {
+      const float x = (q < mc) ? dot_u(q) : 0.0f;
+      v_s[q] = x;
+      __stcg(coef + ent_s[q], x);
+    }
+    if (m > cap) {  // streamed columns: a warp per two columns
       float ur[NW];
 #pragma unroll
       for (int k = 0; k < NW; ++k) {
         const int i = lane + 32 * k;
         ur[k] = (i < n) ? u[i] : 0.0f;
       }
-      for (int q = warp; q < mres; q += kUrWarps) {  // resident columns
-        const float* er = Es + size_t(q) * n4;
-        float ev[NW];
-        float x = 0.0f;
-#pragma unroll
-        for (int k = 0; k < NW; ++k) {
-          const int i = lane + 32 * k;
-          ev[k] = (i < n) ? er[i] : 0.0f;
-          x = fmaf(ur[k], ev[k], x);
-        }
-        x = warp_sum(x);
-        if (q >= mc) x = 0.0f;
-        const int e = ent_s[q];
-        float* rr = R + int64_t(e / L) * n;
-#pragma unroll
-        for (int k = 0; k < NW; ++k) {
-          const int i = lane + 32 * k;
-          if (i < n) __stcg(rr + i, fmaf(-x, ur[k], ev[k]));
-        }
-        if (lane == 0) __stcg(coef + e, x);
-      }
-      for (int q = cap + warp; q < m; q += 2 * kUrWarps) {  // streamed columns
+      for (int q = cap + warp; q < m; q += 2 * kUrWarps) {
         float e0[NW], e1[NW];
         int ea, eb;
         stream_cols(q, m, e0, e1, ea, eb);
@@ -516,6 +580,26 @@ __global__ void __launch_bounds__(kUrThreads, 1)
         }
       }
     }
+    __syncthreads();
+    if (tma) {  // rows of 16-byte aligned float4
+      for (int t = tid; t < mres * F; t += kUrThreads) {
+        const int q = t / F, f = t - q * F;
+        const float x = v_s[q];
+        const float4 e = Es4[size_t(q) * es4 + f], w = u4[f];
+        float4 r;
+        r.x = fmaf(-x, w.x, e.x);
+        r.y = fmaf(-x, w.y, e.y);
+        r.z = fmaf(-x, w.z, e.z);
+        r.w = fmaf(-x, w.w, e.w);
+        __stcg(reinterpret_cast<float4*>(R + int64_t(ent_s[q] / L) * n) + f, r);
+      }
+    } else {
+      for (int t = tid; t < mres * n; t += kUrThreads) {
+        const int q = t / n, i = t - q * n;
+        __stcg(R + int64_t(ent_s[q] / L) * n + i, fmaf(-v_s[q], u[i], Es[size_t(q) * es + i]));
+      }
+    }
+    fence_proxy_async_smem();  // generic accesses of Es before the next bulk copies into it
     __syncthreads();
     if (tid == 0) red_release_add(done_cnt + j, 1u);
     lap(5);
