@@ -93,7 +93,8 @@ struct TcX {
   unsigned long long qmask[kTcQ];   // columns of each quarter inside the error window
   float2 part[kTcQ];                // residual partial norms (all, centred)
   double best, best_b;              // exact best |c| and its d_a . y
-  int best_a, pad;
+  int best_a, ncand;                // its atom; number of candidates this step
+  int noff, pad;                    // offset of the candidates in the tile's list
 };
 
 __host__ __device__ inline size_t tc_al(size_t x, size_t a) { return (x + a - 1) / a * a; }
@@ -230,6 +231,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   TcX* xq = reinterpret_cast<TcX*>(smem + lo.off_xq);
   unsigned long long* mbar = reinterpret_cast<unsigned long long*>(smem + lo.off_bar);
   unsigned* tmem_slot = reinterpret_cast<unsigned*>(smem + lo.off_tmem);
+  // candidate list of the re-score, in the A operand's buffer: |c| and d . y
+  // (FP64), then the packed (patch << 24 | atom) entries
+  const int capl = int((size_t(kTcTile) * lo.np16 * 2) / 20);
+  double* lcs = reinterpret_cast<double*>(At);
+  double* lbs = lcs + capl;
+  int* lpk = reinterpret_cast<int*>(lbs + capl);
+  __shared__ int s_wtot[4];
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int Kp = lo.Kp, np16 = lo.np16, ysn = lo.ysn, tri = lo.tri, qw = lo.qw;
@@ -413,31 +421,82 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         X.qmask[q] = mask;
       }
       __syncthreads();
-      // ---- exact re-score, four consecutive lanes per patch ----------------
-      //   b_a = d_a . y (FP64 from FP32 data),  c_a = b_a - sum_s g_s G[a][s]
+      // ---- exact re-score of every candidate of the tile ------------------
+      // The tile's (patch, atom) candidates form one list, kept in the A
+      // operand's buffer (free between the MMA and the residual update), and
+      // four consecutive lanes score each entry:
+      //   b_a = d_a . y (FP64 from FP32 data),  c_a = b_a - sum_s g_s G[a][s];
+      // each patch then takes its largest |c_a|, lowest atom index on ties.
       {
-        const int ps = tid >> 2, js = tid & 3;
+        if (q == 0) {  // candidate counts and list offsets (warps 0..3)
+          int cntm = 0;
+          if (!done)
+#pragma unroll
+            for (int qq = 0; qq < kTcQ; ++qq) cntm += __popcll(X.qmask[qq]);
+          int incl = cntm;
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+          }
+          if (lane == 31) s_wtot[g] = incl;
+          X.ncand = cntm;
+          X.noff = incl - cntm;
+          X.best = -1.0;
+          X.best_a = 0x7fffffff;
+          X.best_b = 0.0;
+        }
+        __syncthreads();
+        const int total = s_wtot[0] + s_wtot[1] + s_wtot[2] + s_wtot[3];
+        if (q == 0)
+          for (int w = 0; w < g; ++w) X.noff += s_wtot[w];
+        const int grp = tid >> 2, js = tid & 3;
         const unsigned gmask = 0xFu << (lane & ~3);
-        TcX& XS = xq[ps];
-        const float* yrs = Ys + ps * ysn;
-        const int cnt = pp[ps].cnt;
-        double best = -1.0, best_b = 0.0;
-        int best_a = 0x7fffffff;
-        for (int qq = 0; qq < kTcQ; ++qq) {
-          unsigned long long mk = XS.qmask[qq];
-          while (mk) {
-            const int a = qq * qw + (__ffsll((long long)mk) - 1);
-            mk &= mk - 1ull;
+        for (int rb = 0; rb < total; rb += capl) {
+          const int rh = min(total, rb + capl);
+          if (q == 0 && X.ncand > 0 && X.noff < rh && X.noff + X.ncand > rb) {
+            int li = X.noff;  // ascending atom order
+            for (int qq = 0; qq < kTcQ && li < rh; ++qq) {
+              unsigned long long mk = X.qmask[qq];
+              while (mk && li < rh) {
+                const int a = qq * qw + (__ffsll((long long)mk) - 1);
+                mk &= mk - 1ull;
+                if (li >= rb) lpk[li - rb] = (m << 24) | a;
+                ++li;
+              }
+            }
+          }
+          __syncthreads();
+          for (int t = grp; t < rh - rb; t += kTcThreads / 4) {
+            const int v = lpk[t];
+            const int ps = v >> 24, a = v & 0xFFFFFF;
+            const float* yrs = Ys + ps * ysn;
+            const int cnt = pp[ps].cnt;
+            double gs = 0.0;  // support part, lanes js, js + 4, ...
+            for (int s2 = js; s2 < cnt; s2 += 4)
+              gs = fma(double(gam[ps * L + s2]), Gram[int64_t(a) * K + Ss[ps * L + s2]], gs);
             double b0 = 0.0, b1 = 0.0;
             if (d_vec4) {
               const float4* dr = reinterpret_cast<const float4*>(D + int64_t(a) * n);
               const int n4 = n / 4;
-              for (int k4 = js; k4 < n4; k4 += 4) {
-                const float4 d4 = __ldg(dr + k4);
-                b0 = fma(double(d4.x), double(yrs[4 * k4]), b0);
-                b1 = fma(double(d4.y), double(yrs[4 * k4 + 1]), b1);
-                b0 = fma(double(d4.z), double(yrs[4 * k4 + 2]), b0);
-                b1 = fma(double(d4.w), double(yrs[4 * k4 + 3]), b1);
+              for (int k0 = js; k0 < n4; k0 += 16) {
+                float4 dv[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                  const int k4 = k0 + 4 * u;
+                  dv[u] = (k4 < n4) ? __ldg(dr + k4) : make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                  const int k4 = k0 + 4 * u;
+                  if (k4 < n4) {
+                    const float* yv = yrs + 4 * k4;
+                    b0 = fma(double(dv[u].x), double(yv[0]), b0);
+                    b1 = fma(double(dv[u].y), double(yv[1]), b1);
+                    b0 = fma(double(dv[u].z), double(yv[2]), b0);
+                    b1 = fma(double(dv[u].w), double(yv[3]), b1);
+                  }
+                }
               }
             } else {
               for (int k = js; k < n; k += 4) b0 = fma(double(__ldg(D + int64_t(a) * n + k)), double(yrs[k]), b0);
@@ -445,21 +504,28 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             double ba = b0 + b1;
             ba += __shfl_xor_sync(gmask, ba, 1);
             ba += __shfl_xor_sync(gmask, ba, 2);
-            double ca = ba;
-            for (int s2 = 0; s2 < cnt; ++s2) ca -= double(gam[ps * L + s2]) * Gram[int64_t(a) * K + Ss[ps * L + s2]];
-            const double aca = fabs(ca);
-            if (js == 0) ++nscored;
-            if (aca > best || (aca == best && a < best_a)) {
-              best = aca;
-              best_a = a;
-              best_b = ba;
+            gs += __shfl_xor_sync(gmask, gs, 1);
+            gs += __shfl_xor_sync(gmask, gs, 2);
+            if (js == 0) {
+              lcs[t] = fabs(ba - gs);
+              lbs[t] = ba;
+              ++nscored;
             }
           }
-        }
-        if (js == 0) {
-          XS.best = best;
-          XS.best_a = best_a;
-          XS.best_b = best_b;
+          __syncthreads();
+          if (q == 0 && X.ncand > 0) {
+            const int lo = max(X.noff, rb), hi = min(X.noff + X.ncand, rh);
+            for (int t = lo; t < hi; ++t) {
+              const double aca = lcs[t - rb];
+              const int a = lpk[t - rb] & 0xFFFFFF;
+              if (aca > X.best || (aca == X.best && a < X.best_a)) {
+                X.best = aca;
+                X.best_a = a;
+                X.best_b = lbs[t - rb];
+              }
+            }
+          }
+          __syncthreads();
         }
       }
       __syncthreads();
@@ -536,21 +602,40 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             const int kk = kc * 8 + e;
             r[e] = (kk < n) ? yr[kk] : 0.0f;
           }
-          for (int s2 = 0; s2 < cnt; ++s2) {
-            const float gg = gam[m * L + s2];
-            const float* dr = D + int64_t(Ss[m * L + s2]) * n + kc * 8;
-            if (d_vec4 && kc * 8 + 8 <= n) {
-              const float4 d0 = __ldg(reinterpret_cast<const float4*>(dr));
-              const float4 d1 = __ldg(reinterpret_cast<const float4*>(dr) + 1);
-              r[0] = fmaf(-gg, d0.x, r[0]);
-              r[1] = fmaf(-gg, d0.y, r[1]);
-              r[2] = fmaf(-gg, d0.z, r[2]);
-              r[3] = fmaf(-gg, d0.w, r[3]);
-              r[4] = fmaf(-gg, d1.x, r[4]);
-              r[5] = fmaf(-gg, d1.y, r[5]);
-              r[6] = fmaf(-gg, d1.z, r[6]);
-              r[7] = fmaf(-gg, d1.w, r[7]);
-            } else {
+          if (d_vec4 && kc * 8 + 8 <= n) {
+            // the chunk of every support atom is loaded before it is used
+            constexpr int kSB = 2;
+            for (int s0 = 0; s0 < cnt; s0 += kSB) {
+              float4 da[kSB], db[kSB];
+              float gg[kSB];
+#pragma unroll
+              for (int u = 0; u < kSB; ++u) {
+                const int s2 = s0 + u;
+                if (s2 < cnt) {
+                  const float4* dr = reinterpret_cast<const float4*>(D + int64_t(Ss[m * L + s2]) * n + kc * 8);
+                  gg[u] = gam[m * L + s2];
+                  da[u] = __ldg(dr);
+                  db[u] = __ldg(dr + 1);
+                }
+              }
+#pragma unroll
+              for (int u = 0; u < kSB; ++u) {
+                if (s0 + u < cnt) {
+                  r[0] = fmaf(-gg[u], da[u].x, r[0]);
+                  r[1] = fmaf(-gg[u], da[u].y, r[1]);
+                  r[2] = fmaf(-gg[u], da[u].z, r[2]);
+                  r[3] = fmaf(-gg[u], da[u].w, r[3]);
+                  r[4] = fmaf(-gg[u], db[u].x, r[4]);
+                  r[5] = fmaf(-gg[u], db[u].y, r[5]);
+                  r[6] = fmaf(-gg[u], db[u].z, r[6]);
+                  r[7] = fmaf(-gg[u], db[u].w, r[7]);
+                }
+              }
+            }
+          } else {
+            for (int s2 = 0; s2 < cnt; ++s2) {
+              const float gg = gam[m * L + s2];
+              const float* dr = D + int64_t(Ss[m * L + s2]) * n + kc * 8;
 #pragma unroll
               for (int e = 0; e < 8; ++e)
                 if (kc * 8 + e < n) r[e] = fmaf(-gg, __ldg(dr + e), r[e]);
@@ -616,7 +701,7 @@ template __global__ void omp_tc_kernel<true>(const float*, int64_t, int, const f
 
 bool omp_tc_supported(int n, int K, int L) {
   return L >= 1 && L <= kTcLMax && n >= 1 && K >= 1 && tc_al(K, 16) <= 256 &&
-         omp_tc_smem_bytes(n, K, L) <= 232448;
+         omp_tc_smem_bytes(n, K, L) <= 232448 - 256;
 }
 
 cudaError_t launch_omp_tc(const float* patches, int64_t N, int n, const float* dict, const double* gram, int K, int L,
