@@ -150,14 +150,9 @@ ksvd_status validate_params(const ksvd_params* p, std::string* why) {
 }
 
 ksvd_status check_kernel_support(ksvd_ctx* c) {
-  const int n = c->p.patch_width_dim * c->p.patch_height_dim;
-  if (c->p.precision == KSVD_PREC_FP32) {
-    if (!ksvd::omp_fp32_supported(n, c->p.atoms, c->p.omp_iter))
-      return fail(c, KSVD_ERR_INVALID, "patch size x atoms too large for the resident-dictionary OMP kernel");
-  } else {
-    if (!ksvd::omp_tc_supported(n, c->p.atoms, c->p.omp_iter))
-      return fail(c, KSVD_ERR_INVALID, "patch size x atoms too large for the tensor-core OMP kernel");
-  }
+  const int n = c->p.patch_width_dim * c->p.patch_height_dim, K = c->p.atoms, L = c->p.omp_iter;
+  if (!ksvd::omp_tc_supported(n, K, L) && !ksvd::omp_fp32_supported(n, K, L) && !ksvd::omp_stream_supported(n, K, L))
+    return fail(c, KSVD_ERR_INVALID, "patch size x atoms x ompIter beyond every OMP kernel (atoms <= 1024)");
   if (!ksvd::update_res_supported(n))
     return fail(c, KSVD_ERR_INVALID, "patch size > 512 not supported by the update kernel");
   return KSVD_OK;
@@ -403,17 +398,22 @@ static ksvd_status omp_impl(ksvd_ctx* c, const float* d_patches, int64_t N, cons
     KSVD_CU(c, ksvd::launch_gram_f64(d_dict, K, n, gram, c->stream), "gram");
   }
   Prof pr(c, "omp", 1);
-  if (c->p.precision != KSVD_PREC_FP32) {
+  ksvd::DevStats* ph = c->profiling >= 2 ? c->d_phase : nullptr;
+  // The tensor-core forms need the 16-bit dictionary in shared memory (atoms
+  // <= 256); beyond that, and for the FP32 form, the FP32 kernels run: the
+  // resident-dictionary one when it fits, else the streamed one.
+  if (c->p.precision != KSVD_PREC_FP32 && ksvd::omp_tc_supported(n, K, L)) {
     KSVD_CU(c,
             ksvd::launch_omp_tc(d_patches, N, n, d_dict, gram, K, L, d_idx, d_coef, c->num_sms,
-                                c->p.precision == KSVD_PREC_FP16_RESCORE ? 1 : 0, c->d_flags,
-                                c->profiling >= 2 ? c->d_phase : nullptr, c->stream),
+                                c->p.precision == KSVD_PREC_FP16_RESCORE ? 1 : 0, c->d_flags, ph, c->stream),
             "omp (tensor cores)");
+  } else if (ksvd::omp_fp32_supported(n, K, L)) {
+    KSVD_CU(c, ksvd::launch_omp_fp32(d_patches, N, n, d_dict, gram, K, L, d_idx, d_coef, c->num_sms, ph, c->stream),
+            "omp");
   } else {
     KSVD_CU(c,
-            ksvd::launch_omp_fp32(d_patches, N, n, d_dict, gram, K, L, d_idx, d_coef, c->num_sms,
-                                  c->profiling >= 2 ? c->d_phase : nullptr, c->stream),
-            "omp");
+            ksvd::launch_omp_stream(d_patches, N, n, d_dict, gram, K, L, d_idx, d_coef, c->num_sms, ph, c->stream),
+            "omp (streamed dictionary)");
   }
   return KSVD_OK;
 }
@@ -424,8 +424,7 @@ ksvd_status ksvd_omp(ksvd_ctx* c, const float* d_patches, int64_t N, const float
   if (!d_patches || !d_dict || !d_idx || !d_coef || N < 1) return fail(c, KSVD_ERR_INVALID, "bad argument");
   KSVD_TRY(check_kernel_support(c));
   KSVD_TRY(omp_impl(c, d_patches, N, d_dict, d_idx, d_coef));
-  if (c->p.precision != KSVD_PREC_FP32) return check_dev_flags(c, "omp");
-  return KSVD_OK;
+  return check_dev_flags(c, "omp");
 }
 
 static ksvd_status update_impl(ksvd_ctx* c, const float* d_patches, int64_t N, float* d_dict, const int32_t* d_idx,

@@ -74,6 +74,12 @@ cudaError_t launch_omp_fp32(const float* patches, int64_t N, int n, const float*
                             int K, int L, int32_t* idx, float* coef, int num_sms, DevStats* stats,
                             cudaStream_t s);
 
+// OMP (FP32 SIMT) with the dictionary streamed through shared memory in
+// feature chunks: any K <= 1024 and n as long as one 4-feature chunk fits.
+bool omp_stream_supported(int n, int K, int L);
+cudaError_t launch_omp_stream(const float* patches, int64_t N, int n, const float* dict, const double* gram, int K,
+                              int L, int32_t* idx, float* coef, int num_sms, DevStats* stats, cudaStream_t s);
+
 // OMP with the BF16 tensor-core correlation and exact FP32/FP64 re-scoring.
 size_t omp_tc_smem_bytes(int n, int K, int L);
 bool omp_tc_supported(int n, int K, int L);

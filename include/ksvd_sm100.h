@@ -70,7 +70,11 @@ typedef enum ksvd_status {
  * lies within the operand-rounding error bound of the best one, so the
  * selected atom is the exact argmax either way; FP16 (11-bit significand,
  * exact power-of-two scaling per patch) gives an 8x narrower bound than BF16
- * and therefore far fewer re-scores. */
+ * and therefore far fewer re-scores.
+ * The tensor-core forms apply for atoms <= 256 when the tile of 128 patches
+ * and the 16-bit dictionary fit in shared memory; beyond that the FP32
+ * kernels run (dictionary resident in shared memory when it fits, streamed
+ * through it otherwise: atoms <= 1024). */
 typedef enum ksvd_precision {
   KSVD_PREC_FP32 = 0,         /* plain FP32 FMA                              */
   KSVD_PREC_BF16_RESCORE = 1, /* BF16 tensor cores + exact re-score         */
