@@ -535,30 +535,60 @@ ksvd_status ksvd_codes_to_dense(ksvd_ctx* c, const int32_t* d_idx, const float* 
 // ---------------------------------------------------------------------------
 // Whole denoise (host buffers)
 // ---------------------------------------------------------------------------
+// The K-SVD pipeline on one device image y (log2 domain for speckle): patch
+// gather, initial dictionary, ksvd_iter x (OMP + update), final OMP and the
+// rebuild into d_out (exp2 applied for speckle).  ev[0..5] (may be null)
+// bracket gather, set-up, iterations, final OMP and rebuild.
+static ksvd_status denoise_image(ksvd_ctx* c, const float* y, int width, int height, float sigma2, float* d_out,
+                                 double* lam, int64_t* npatch, cudaEvent_t* ev) {
+  PatchGeom g;
+  if (!geom_of(c->p, width, height, &g)) return fail(c, KSVD_ERR_INVALID, "patch geometry does not fit the image");
+  const int n = g.n, K = c->p.atoms, L = c->p.omp_iter;
+  if (g.N / 2 + K > g.N) return fail(c, KSVD_ERR_INVALID, "fewer patches than N/2 + atoms");
+  float *d_patches = nullptr, *d_dict = nullptr, *d_coef = nullptr;
+  int32_t* d_idx = nullptr;
+  KSVD_TRY(wsT(c, "den_patches", size_t(g.N) * n, &d_patches));
+  KSVD_TRY(wsT(c, "den_dict", size_t(K) * n, &d_dict));
+  KSVD_TRY(wsT(c, "den_idx", size_t(g.N) * L, &d_idx));
+  KSVD_TRY(wsT(c, "den_coef", size_t(g.N) * L, &d_coef));
+  auto mark = [&](int i) {
+    if (ev) cudaEventRecord(ev[i], c->stream);
+  };
+  mark(0);
+  ksvd_status st = ksvd_extract_patches(c, y, width, height, d_patches);
+  mark(1);
+  if (st == KSVD_OK) st = ksvd_init_dictionary(c, d_patches, g.N, d_dict);
+  mark(2);
+  for (int i = 0; st == KSVD_OK && i < c->p.ksvd_iter; ++i) {
+    st = omp_impl(c, d_patches, g.N, d_dict, d_idx, d_coef);
+    if (st == KSVD_OK) st = update_impl(c, d_patches, g.N, d_dict, d_idx, d_coef);
+  }
+  mark(3);
+  if (st == KSVD_OK) st = omp_impl(c, d_patches, g.N, d_dict, d_idx, d_coef);
+  mark(4);
+  if (st == KSVD_OK) st = ksvd_build_image(c, y, width, height, sigma2, d_dict, d_idx, d_coef, g.N, d_out, lam);
+  mark(5);
+  *npatch = g.N;
+  return st;
+}
+
 ksvd_status ksvd_denoise(ksvd_ctx* c, const float* img, int width, int height, float sigma2, float* out,
                          ksvd_stats* stats) {
   using clk = std::chrono::steady_clock;
   KSVD_TRY(check_ctx(c));
   if (!img || !out) return fail(c, KSVD_ERR_INVALID, "null image pointer");
+  if (width < 1 || height < 1) return fail(c, KSVD_ERR_INVALID, "empty image");
   if (!(sigma2 > 0.0f)) return fail(c, KSVD_ERR_INVALID, "sigma2 must be > 0");
-  if (c->p.sub_image_width_dim != 0 || c->p.sub_image_height_dim != 0)
-    return fail(c, KSVD_ERR_INVALID, "sub-image tiling is not available in this build");
   KSVD_TRY(check_kernel_support(c));
-  PatchGeom g;
-  if (!geom_of(c->p, width, height, &g)) return fail(c, KSVD_ERR_INVALID, "patch geometry does not fit the image");
-  const int n = g.n, K = c->p.atoms, L = c->p.omp_iter;
-  if (g.N / 2 + K > g.N) return fail(c, KSVD_ERR_INVALID, "fewer patches than N/2 + atoms");
+  const int tw = c->p.sub_image_width_dim, th = c->p.sub_image_height_dim;
+  const bool tiled = tw != 0 || th != 0;
+  if (tiled && (tw < 1 || th < 1 || th > width || tw > height))
+    return fail(c, KSVD_ERR_INVALID, "sub-image dimensions do not fit the image");
   const size_t P = size_t(width) * height;
-  float *d_img = nullptr, *d_y = nullptr, *d_patches = nullptr, *d_dict = nullptr, *d_coef = nullptr,
-        *d_out = nullptr;
-  int32_t* d_idx = nullptr;
+  float *d_img = nullptr, *d_y = nullptr, *d_out = nullptr;
   KSVD_TRY(wsT(c, "den_img", P, &d_img));
   KSVD_TRY(wsT(c, "den_y", P, &d_y));
   KSVD_TRY(wsT(c, "den_out", P, &d_out));
-  KSVD_TRY(wsT(c, "den_patches", size_t(g.N) * n, &d_patches));
-  KSVD_TRY(wsT(c, "den_dict", size_t(K) * n, &d_dict));
-  KSVD_TRY(wsT(c, "den_idx", size_t(g.N) * L, &d_idx));
-  KSVD_TRY(wsT(c, "den_coef", size_t(g.N) * L, &d_coef));
   cudaEvent_t ev[6];
   for (auto& e : ev) e = get_event(c);
   auto release = [&]() {
@@ -572,22 +602,47 @@ ksvd_status ksvd_denoise(ksvd_ctx* c, const float* img, int width, int height, f
     KSVD_CU(c, ksvd::launch_log2_image(d_img, d_y, int64_t(P), c->stream), "log2");
     y = d_y;
   }
-  cudaEventRecord(ev[0], c->stream);
-  ksvd_status st = ksvd_extract_patches(c, y, width, height, d_patches);
-  cudaEventRecord(ev[1], c->stream);
-  if (st == KSVD_OK) st = ksvd_init_dictionary(c, d_patches, g.N, d_dict);
   const auto t1 = clk::now();
-  cudaEventRecord(ev[2], c->stream);
-  for (int i = 0; st == KSVD_OK && i < c->p.ksvd_iter; ++i) {
-    st = omp_impl(c, d_patches, g.N, d_dict, d_idx, d_coef);
-    if (st == KSVD_OK) st = update_impl(c, d_patches, g.N, d_dict, d_idx, d_coef);
-  }
-  cudaEventRecord(ev[3], c->stream);
-  if (st == KSVD_OK) st = omp_impl(c, d_patches, g.N, d_dict, d_idx, d_coef);
-  cudaEventRecord(ev[4], c->stream);
+  ksvd_status st = KSVD_OK;
   double lam = 0.0;
-  if (st == KSVD_OK) st = ksvd_build_image(c, y, width, height, sigma2, d_dict, d_idx, d_coef, g.N, d_out, &lam);
-  cudaEventRecord(ev[5], c->stream);
+  int64_t npatch = 0;
+  if (!tiled) {
+    st = denoise_image(c, y, width, height, sigma2, d_out, &lam, &npatch, ev);
+  } else {
+    // Sub-image mode (cuda_svd_denoiser.cu:130-188, 503-528): the image is cut
+    // into non-overlapping sub-images of subImageHeightDim (along x) by
+    // subImageWidthDim (along y), the patch convention, at a step of their own
+    // size; each is denoised on its own (own dictionary) and written back in
+    // place.  Pixels outside the complete sub-images are returned as input.
+    KSVD_CU(c, cudaMemcpyAsync(d_out, d_img, P * sizeof(float), cudaMemcpyDeviceToDevice, c->stream), "copy");
+    float *d_tin = nullptr, *d_tout = nullptr;
+    KSVD_TRY(wsT(c, "den_tile_in", size_t(tw) * th, &d_tin));
+    KSVD_TRY(wsT(c, "den_tile_out", size_t(tw) * th, &d_tout));
+    const int nx = (width - th) / th + 1, ny = (height - tw) / tw + 1;
+    for (int i : {0, 1, 2}) cudaEventRecord(ev[i], c->stream);
+    double lsum = 0.0;
+    for (int ix = 0; st == KSVD_OK && ix < nx; ++ix) {
+      for (int iy = 0; st == KSVD_OK && iy < ny; ++iy) {
+        const size_t off = size_t(iy) * tw * width + size_t(ix) * th;
+        KSVD_CU(c,
+                cudaMemcpy2DAsync(d_tin, size_t(th) * 4, y + off, size_t(width) * 4, size_t(th) * 4, tw,
+                                  cudaMemcpyDeviceToDevice, c->stream),
+                "sub-image gather");
+        double lt = 0.0;
+        int64_t nt = 0;
+        st = denoise_image(c, d_tin, th, tw, sigma2, d_tout, &lt, &nt, nullptr);
+        if (st != KSVD_OK) break;
+        KSVD_CU(c,
+                cudaMemcpy2DAsync(d_out + off, size_t(width) * 4, d_tout, size_t(th) * 4, size_t(th) * 4, tw,
+                                  cudaMemcpyDeviceToDevice, c->stream),
+                "sub-image scatter");
+        lsum += lt;
+        npatch += nt;
+      }
+    }
+    lam = lsum / double(nx * ny);
+    for (int i : {3, 4, 5}) cudaEventRecord(ev[i], c->stream);
+  }
   if (st == KSVD_OK) st = check_dev_flags(c, "denoise");
   const auto t2 = clk::now();
   if (st == KSVD_OK) {
@@ -604,11 +659,12 @@ ksvd_status ksvd_denoise(ksvd_ctx* c, const float* img, int width, int height, f
     stats->init_ms = ms(t0, t1);
     stats->working_ms = ms(t1, t2);
     stats->finalize_ms = ms(t2, t3);
-    stats->num_patches = g.N;
+    stats->num_patches = npatch;
     stats->lambda = lam;
     float f = 0.0f;
     cudaEventElapsedTime(&f, ev[0], ev[1]);
     stats->extract_ms = f;
+    // sub-image mode: the whole sub-image loop counts as iterations
     cudaEventElapsedTime(&f, ev[2], ev[3]);
     stats->iter_ms = f;
     cudaEventElapsedTime(&f, ev[3], ev[4]);

@@ -194,6 +194,24 @@ if os.environ.get("KSVD_ORACLE_THREADS"):
     set_threads(int(os.environ["KSVD_ORACLE_THREADS"]))
 
 
+def ksvd_denoise_tiled(noisy: np.ndarray, sigma2: float, sub_w: int, sub_h: int, **kw):
+    """Sub-image mode (cuda_svd_denoiser.cu:130-188, 503-528): non-overlapping
+    sub-images of sub_h (along x, the column index) by sub_w (along y, the
+    row index) at a step of their own size, each denoised on its own with the
+    same sigma2; pixels outside the complete sub-images are returned as the
+    input.  Returns (image, mean lambda)."""
+    H, W = noisy.shape
+    out = np.array(noisy, dtype=np.float32, copy=True)
+    lams = []
+    for x0 in range(0, W - sub_h + 1, sub_h):
+        for y0 in range(0, H - sub_w + 1, sub_w):
+            tile = np.ascontiguousarray(noisy[y0:y0 + sub_w, x0:x0 + sub_h])
+            r, info = ksvd_denoise(tile, sigma2, **kw)
+            out[y0:y0 + sub_w, x0:x0 + sub_h] = r
+            lams.append(info["lambda"])
+    return out, float(np.mean(lams))
+
+
 def compact_to_dense(idx: np.ndarray, coef: np.ndarray, K: int) -> np.ndarray:
     """Compact codes (N, L) -> dense (N, K); unused slots (idx < 0) skipped."""
     N, L = idx.shape

@@ -296,3 +296,34 @@ def test_denoise_img512_workload_vs_fp64_oracle(torch_cuda, ksvd, oracle, synth,
                                  omp_iter=5, q1_cap=True, int_norm=True)
     pg, pr = synth.psnr(clean, out), synth.psnr(clean, ref)
     assert abs(pg - pr) <= 0.05, (pg, pr)
+
+
+@pytest.mark.parametrize("precision", [0, 2])
+def test_denoise_subimages_vs_fp64_oracle(torch_cuda, ksvd, oracle, synth, precision):
+    """Sub-image mode: a 128 (x) x 100 (y) image cut into 60 x 48 sub-images
+    (2 x 2 of them), each denoised with its own dictionary; the 8-pixel strip
+    at the right and the 4 rows at the bottom are outside every sub-image and
+    come back unchanged.  PSNR within 0.05 dB of the FP64 oracle."""
+    clean = synth.clean_image(128, 51)[:100, :]
+    noisy = synth.add_gaussian(clean, 20.0, 51)
+    kw = dict(patch_width_dim=8, patch_height_dim=8, sliding_width=2, sliding_height=2, atoms=64, omp_iter=5,
+              ksvd_iter=2, compat=1, precision=precision, sub_image_width_dim=48, sub_image_height_dim=60)
+    with mkctx(ksvd, **kw) as c:
+        out, st = c.denoise(noisy, 400.0)
+    ref, lam = oracle.ksvd_denoise_tiled(noisy, 400.0, 48, 60, pw=8, ph=8, sw=2, sh=2, atoms=64, ksvd_iter=2,
+                                         omp_iter=5, q1_cap=False, int_norm=True)
+    np.testing.assert_array_equal(out[:, 120:], noisy[:, 120:])
+    np.testing.assert_array_equal(out[96:, :], noisy[96:, :])
+    pg, pr = synth.psnr(clean[:96, :120], out[:96, :120]), synth.psnr(clean[:96, :120], ref[:96, :120])
+    assert abs(pg - pr) <= 0.05, (pg, pr)
+    assert pg > synth.psnr(clean[:96, :120], noisy[:96, :120]) + 2.0
+    assert st["num_patches"] == 4 * 27 * 21
+    assert st["lambda_"] == pytest.approx(lam, rel=1e-2)
+
+
+def test_subimage_errors(torch_cuda, ksvd, synth):
+    img = synth.clean_image(64, 2)
+    with mkctx(ksvd, atoms=16, sub_image_width_dim=80, sub_image_height_dim=32) as c:
+        with pytest.raises(ksvd.KsvdError) as e:
+            c.denoise(img, 100.0)
+        assert e.value.status == ksvd.ERR_INVALID
