@@ -119,6 +119,28 @@ def dist_env():
     return rank, world, local
 
 
+def replica_workload(wl, rank):
+    """Rank r denoises its own image: the workload with seed + r (replicas,
+    no data exchanged between ranks)."""
+    from dataclasses import replace
+    return replace(wl, seed=wl.seed + rank)
+
+
+def reduce_max(x, dist, device="cpu"):
+    """Maximum of a per-rank float over all ranks (x itself without a group)."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(units_per_rank, world, ms_max):
+    """Whole-job rate: the units all ranks processed over the slowest rank's time."""
+    return units_per_rank * world / (ms_max / 1000.0)
+
+
 def _cpu_sample_size(oracle, Y, D, wl, budget_s):
     """Patches per timed CPU iteration: the whole workload when one iteration
     is estimated to fit the budget, else a contiguous middle slice sized for it.
@@ -248,8 +270,7 @@ def main():
     ctx, params = make_ctx(args.precision)
 
     # each rank: its own seeded image (replicas)
-    from dataclasses import replace
-    wlr = replace(wl, seed=wl.seed + rank)
+    wlr = replica_workload(wl, rank)
     clean, noisy = wlr.images()
     H, W = noisy.shape
     N = ksvd.num_patches(params, W, H)
@@ -308,15 +329,12 @@ def main():
         ph = c.profile_phases()
         cn.update({k: v for k, v in c.profile_counters().items() if k.startswith("omp_")})
         c.profile(0)
-        if dist:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = reduce_max(ms, dist, "cuda")
         return ms, fams, ph, cn, c.launch_count() - l0, (sampler.summary() if sampler else None)
 
     # ---- the headline form: warm-up, then K timed K-SVD iterations ---------
     ms_step, fam, phases, counters, gpu_launches, clk_summary = timed_steps(ctx, True)
-    value = N * world / (ms_step / 1000.0)
+    value = aggregate_rate(N, world, ms_step)
     forms = {args.precision: value}
     if not args.no_forms:
         for form in ("fp32", "fp16", "bf16"):
@@ -324,7 +342,7 @@ def main():
                 continue
             c2, _ = make_ctx(form)
             ms2 = timed_steps(c2, False)[0]
-            forms[form] = N * world / (ms2 / 1000.0)
+            forms[form] = aggregate_rate(N, world, ms2)
             c2.close()
 
     # ---- e2e through the C ABI with pinned host buffers --------------------
@@ -341,11 +359,8 @@ def main():
         if i > 0:  # first call is a warm-up
             e2e_ms.append(e0.elapsed_time(e1))
     e2e_call_ms = float(np.median(e2e_ms))
-    if dist:
-        t = torch.tensor([e2e_call_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_call_ms = float(t.item())
-    e2e_value = N * wl.ksvd_iter * world / (e2e_call_ms / 1000.0)
+    e2e_call_ms = reduce_max(e2e_call_ms, dist, "cuda")
+    e2e_value = aggregate_rate(N * wl.ksvd_iter, world, e2e_call_ms)
     out = out_h.numpy()
     psnr_noisy = pkg.synth.psnr(clean, noisy)
     psnr_out = pkg.synth.psnr(clean, out)
