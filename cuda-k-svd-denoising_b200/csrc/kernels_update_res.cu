@@ -86,23 +86,69 @@ __host__ __device__ inline int ur_active(int c, int G) {
   return a < G ? a : G;
 }
 
-// residual_kernel: R = Y - X D, one warp per patch (the code slots are read
-// by every lane of the warp: uniform, cached loads).
+// residual_kernel: R = Y - X D, one warp per patch.  The patch's atoms and
+// coefficients sit in lanes 0..L-1 and are broadcast by shuffles; each lane
+// forms 16-byte pieces of the row with the support atoms' loads in flight
+// together (same FMA order as r = y - sum_s x_s d_s, s ascending).
 __global__ void __launch_bounds__(256) residual_kernel(const float* __restrict__ Y, int64_t N, int n,
                                                        const float* __restrict__ D, int K, int L,
                                                        const int32_t* __restrict__ idx,
-                                                       const float* __restrict__ coef, float* __restrict__ R) {
+                                                       const float* __restrict__ coef, float* __restrict__ R,
+                                                       int vec4) {
   const int lane = threadIdx.x & 31;
   const int64_t warps = int64_t(gridDim.x) * (blockDim.x >> 5);
   for (int64_t p = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); p < N; p += warps) {
-    for (int i = lane; i < n; i += 32) {
-      float r = Y[p * n + i];
-      for (int s = 0; s < L; ++s) {
-        const int a = __ldg(idx + p * L + s);
-        const float x = __ldg(coef + p * L + s);
-        if (a >= 0 && a < K && x != 0.0f) r = fmaf(-x, __ldg(D + int64_t(a) * n + i), r);
+    int a = -1;
+    float x = 0.0f;
+    if (lane < L) {
+      a = __ldg(idx + p * L + lane);
+      x = __ldg(coef + p * L + lane);
+      if (a < 0 || a >= K || x == 0.0f) a = -1;
+    }
+    if (vec4) {
+      const int F = n >> 2;
+      const float4* y4 = reinterpret_cast<const float4*>(Y + p * n);
+      float4* r4 = reinterpret_cast<float4*>(R + p * n);
+      for (int f0 = 0; f0 < F; f0 += 32) {
+        const int f = f0 + lane;
+        const bool in = f < F;
+        float4 r = in ? __ldg(y4 + f) : make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int s0 = 0; s0 < L; s0 += 8) {
+          float4 dv[8];
+          float xs[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            const int as = __shfl_sync(0xffffffffu, a, (s0 + u) & 31);
+            xs[u] = __shfl_sync(0xffffffffu, x, (s0 + u) & 31);
+            const bool use = in && s0 + u < L && as >= 0;
+            dv[u] = use ? __ldg(reinterpret_cast<const float4*>(D + int64_t(as) * n) + f)
+                        : make_float4(0.f, 0.f, 0.f, 0.f);
+            if (!use) xs[u] = 0.0f;
+          }
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            if (xs[u] != 0.0f) {
+              r.x = fmaf(-xs[u], dv[u].x, r.x);
+              r.y = fmaf(-xs[u], dv[u].y, r.y);
+              r.z = fmaf(-xs[u], dv[u].z, r.z);
+              r.w = fmaf(-xs[u], dv[u].w, r.w);
+            }
+          }
+        }
+        if (in) r4[f] = r;
       }
-      R[p * n + i] = r;
+    } else {
+      for (int i0 = 0; i0 < n; i0 += 32) {
+        const int i = i0 + lane;
+        const bool in = i < n;
+        float r = in ? Y[p * n + i] : 0.0f;
+        for (int s = 0; s < L; ++s) {
+          const int as = __shfl_sync(0xffffffffu, a, s & 31);
+          const float xs = __shfl_sync(0xffffffffu, x, s & 31);
+          if (in && as >= 0) r = fmaf(-xs, __ldg(D + int64_t(as) * n + i), r);
+        }
+        if (in) R[p * n + i] = r;
+      }
     }
   }
 }
@@ -661,7 +707,11 @@ cudaError_t launch_residual(const float* Y, int64_t N, int n, const float* D, in
                             const float* coef, float* R, int num_sms, cudaStream_t s) {
   const int64_t want = (N + 7) / 8;
   const int blocks = int(want < int64_t(num_sms) * 16 ? want : int64_t(num_sms) * 16);
-  residual_kernel<<<blocks > 0 ? blocks : 1, 256, 0, s>>>(Y, N, n, D, K, L, idx, coef, R);
+  const int vec4 = ((n & 3) == 0 && (reinterpret_cast<uintptr_t>(Y) & 15) == 0 &&
+                    (reinterpret_cast<uintptr_t>(D) & 15) == 0 && (reinterpret_cast<uintptr_t>(R) & 15) == 0)
+                       ? 1
+                       : 0;
+  residual_kernel<<<blocks > 0 ? blocks : 1, 256, 0, s>>>(Y, N, n, D, K, L, idx, coef, R, vec4);
   return cudaGetLastError();
 }
 
