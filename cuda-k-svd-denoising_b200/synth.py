@@ -100,4 +100,7 @@ WORKLOADS = {
     "img512_p12s3_k256": Workload("img512_p12s3_k256", 512, 20.0, 12, 3, 256, 5, 10),
     "img2048_p12s3_k256": Workload("img2048_p12s3_k256", 2048, 25.0, 12, 3, 256, 5, 10),
     "img4096_p16s2_k512": Workload("img4096_p16s2_k512", 4096, 15.0, 16, 2, 512, 8, 8),
+    # profiling case: the 2048^2 shape at 1536^2 (259,081 patches, a 149 MB
+    # patch matrix: larger than L2, a few hundred MB on the device)
+    "img1536_p12s3_k256": Workload("img1536_p12s3_k256", 1536, 25.0, 12, 3, 256, 5, 10),
 }
