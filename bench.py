@@ -400,7 +400,7 @@ def main():
             "config": {"workload": wl.name, "image": f"{wl.size}x{wl.size}", "sigma": wl.sigma,
                        "patch": f"{wl.patch}x{wl.patch}", "stride": wl.stride, "num_patches": N, "atoms": K,
                        "omp_iter": L, "precision": args.precision, "compat": args.compat,
-                       "l2": "inputs larger than L2 (265 MB patch matrix), no flush",
+                       "l2": f"inputs larger than L2 ({N * n * 4 / 1e6:.0f} MB patch matrix), no flush",
                        "parallelism": f"replicas x{world}"},
             "e2e": {"value": e2e_value, "unit": "patches/s", "h2d_bytes_per_step": int(W * H * 4),
                     "d2h_bytes_per_step": int(W * H * 4), "ms_per_call": e2e_call_ms,
