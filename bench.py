@@ -414,7 +414,7 @@ def main():
                 name: phases[i] for i, name in (
                     (7, "upd_setup"), (0, "upd_wait_prev_atom"), (1, "upd_load"), (2, "upd_pass"),
                     (3, "upd_wait_partials"), (4, "upd_allreduce"), (5, "upd_coef_store"), (8, "omp_corr"),
-                    (9, "omp_ls"), (10, "omp_io"), (11, "omp_rescore"))},
+                    (9, "omp_residual"), (10, "omp_io"), (11, "omp_rescore"), (12, "omp_cholesky"))},
             "counters_per_step": {k: (v if k.startswith("omp_") else v / max(args.steps, 1))
                                   for k, v in counters.items()},
             "quality": {"psnr_noisy": psnr_noisy, "psnr_denoised": psnr_out,

@@ -294,10 +294,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   auto Lat = [&](int i, int j) -> double& { return Lp[i * (i + 1) / 2 + j]; };
 
   const bool timer = (blockIdx.x == 0 && tid == 0 && stats != nullptr);
-  // phase times (slots 8..11) gather in shared memory, flushed once at the end
-  __shared__ unsigned long long s_ph[4];
+  // phase times (slots 8..12) gather in shared memory, flushed once at the end
+  __shared__ unsigned long long s_ph[5];
   if (timer)
-    for (int k = 0; k < 4; ++k) s_ph[k] = 0ull;
+    for (int k = 0; k < 5; ++k) s_ph[k] = 0ull;
   unsigned long long tmark = timer ? globaltimer_ns() : 0ull;
   auto lap = [&](int slot) {
     if (timer) {
@@ -589,6 +589,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         if (stop) P.done = 1;
       }
       __syncthreads();
+      lap(12);
       // ---- residual quarter (FP32), partial norms, next A operand -----------
       const bool live = !done && !P.done;
       float nrm = 0.0f, cn = 0.0f;
@@ -681,7 +682,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   }
   if (stats && nscored) atomicAdd(&stats->pad, (unsigned long long)nscored);
   if (timer)
-    for (int k = 0; k < 4; ++k) atomicAdd(&stats->phase_ns[8 + k], s_ph[k]);
+    for (int k = 0; k < 5; ++k) atomicAdd(&stats->phase_ns[8 + k], s_ph[k]);
   // ---- teardown --------------------------------------------------------------
   if (failed && tid == 0) mbar_wait(mbar, phase, kMmaWaitNs);  // bounded drain of MMAs in flight
   tc_fence_before();

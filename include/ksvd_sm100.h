@@ -219,8 +219,9 @@ int64_t ksvd_launch_count(const ksvd_ctx* ctx);
  * [0] wait for the previous atom, [1] column load, [2] local power pass,
  * [3] wait for the other CTAs' partials, [4] partial all-reduce and
  * normalisation, [5] coefficients and residual store; OMP [8] correlation +
- * argmax, [9] least squares + residual, [10] tile load/store, [11] exact
- * re-scores.  Synchronises the stream. */
+ * argmax, [9] residual update (least squares included for the FP32 kernels),
+ * [10] tile load/store, [11] exact re-scores, [12] Cholesky append and solve
+ * (tensor-core kernel).  Synchronises the stream. */
 ksvd_status ksvd_profile_phases(ksvd_ctx* ctx, double* ms_out, int count);
 /* Counters accumulated while profiling: [0] power iterations, [1] atoms
  * updated (level >= 1), [2] tensor-core OMP error windows wider than its
