@@ -92,3 +92,22 @@ def test_denoise_large_shapes_vs_fp64_oracle(torch_cuda, ksvd, oracle, synth, pw
                                  q1_cap=False, int_norm=True)
     pg, pr = synth.psnr(clean, out), synth.psnr(clean, ref)
     assert abs(pg - pr) <= 0.05, (pg, pr)
+
+
+@pytest.mark.parametrize("side,pw,K,speckle", [(96, 8, 64, False), (112, 12, 128, True), (128, 22, 64, False)])
+def test_uneven_images_vs_fp64_oracle(torch_cuda, ksvd, oracle, synth, side, pw, K, speckle):
+    """Images of the uneven multi-image workload's kinds (8x8, 12x12 and 22x22
+    patches at stride 3, Gaussian or speckle noise), one context each, against
+    the FP64 oracle."""
+    clean = synth.clean_image(side, 60 + pw) + (1.0 if speckle else 0.0)
+    noisy = synth.add_speckle(clean, 4.0, 60 + pw) if speckle else synth.add_gaussian(clean, 30.0, 60 + pw)
+    sigma2 = 0.3 if speckle else 900.0
+    kw = dict(patch_width_dim=pw, patch_height_dim=pw, sliding_width=3, sliding_height=3, atoms=K, omp_iter=5,
+              ksvd_iter=1, compat=1, speckle=int(speckle))
+    with mkctx(ksvd, **kw) as c:
+        out, _ = c.denoise(noisy, sigma2)
+    ref, _ = oracle.ksvd_denoise(noisy, sigma2, pw=pw, ph=pw, sw=3, sh=3, atoms=K, ksvd_iter=1, omp_iter=5,
+                                 speckle=speckle, q1_cap=False, int_norm=True)
+    assert np.all(np.isfinite(out))
+    pg, pr = synth.psnr(clean, out), synth.psnr(clean, ref)
+    assert abs(pg - pr) <= 0.05, (pg, pr)
