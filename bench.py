@@ -9,7 +9,9 @@ stride 3 (679^2 = 461,041 patches of 144 values), 256 atoms, OMP limited to
 A "step" is one K-SVD iteration over all patches (kSvd's loop body,
 cuda_svd_denoiser.cu:374-397).  value = patches x steps / device time of the
 steps (max over ranks), inputs resident in HBM.  The patch matrix (265 MB) is
-larger than L2, so no explicit flush is needed between steps.
+larger than L2, so no explicit flush is needed between steps; workloads
+whose patch and residual matrices fit in L2 are timed step by step with an
+L2 flush (a write larger than L2) before each step.
 
 e2e = the same metric through the C ABI's ksvd_denoise with host buffers
 (pinned): H2D of the image, patch gather, dictionary init, all iterations,
@@ -287,6 +289,15 @@ def main():
     ctx.extract_patches(img_d, patches)
     ctx.init_dictionary(patches, D)
     D0 = D.clone()
+    # the step's working set is the patch matrix plus the residual matrix of
+    # the same size; below the L2 size (126 MB) steps are timed one by one
+    # with an L2 flush between them
+    l2_bytes = 126 * 1024 * 1024
+    fits_l2 = 2 * N * n * 4 < l2_bytes
+    flush_buf = None
+    if fits_l2:
+        with torch.cuda.stream(stream):
+            flush_buf = torch.zeros(2 * l2_bytes // 4, dtype=torch.float32, device="cuda")
     stream.synchronize()
 
     def timed_steps(c, sample_clocks):
@@ -303,23 +314,34 @@ def main():
         c.profile(1)
         c.profile_reset()
         l0 = c.launch_count()
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(args.steps if flush_buf is not None else 1)]
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
         sampler = ClockSampler(local) if sample_clocks else None
         if sampler:
             sampler.__enter__()
-        ev0.record(stream)
-        for _ in range(args.steps):
-            c.iterate(patches, D, idx, coef, 1)
-        ev1.record(stream)
+        if flush_buf is None:
+            evs[0][0].record(stream)
+            for _ in range(args.steps):
+                c.iterate(patches, D, idx, coef, 1)
+            evs[0][1].record(stream)
+        else:
+            # inputs fit in L2: each step is timed alone, after a write of a
+            # buffer larger than L2 (outside the step's events)
+            for e0, e1 in evs:
+                with torch.cuda.stream(stream):
+                    flush_buf.add_(1)
+                e0.record(stream)
+                c.iterate(patches, D, idx, coef, 1)
+                e1.record(stream)
         torch.cuda.synchronize()
         if sampler:
             sampler.__exit__(None, None, None)
         if dist:
             dist.barrier()
-        ms = ev0.elapsed_time(ev1) / args.steps
+        ms = sum(e0.elapsed_time(e1) for e0, e1 in evs) / args.steps
         fams = {f: c.profile_read(f) for f in ("gram", "omp", "csr", "residual", "update")}
         cn = c.profile_counters()
         # one more (untimed) iteration with the in-kernel phase timers on
@@ -400,7 +422,10 @@ def main():
             "config": {"workload": wl.name, "image": f"{wl.size}x{wl.size}", "sigma": wl.sigma,
                        "patch": f"{wl.patch}x{wl.patch}", "stride": wl.stride, "num_patches": N, "atoms": K,
                        "omp_iter": L, "precision": args.precision, "compat": args.compat,
-                       "l2": f"inputs larger than L2 ({N * n * 4 / 1e6:.0f} MB patch matrix), no flush",
+                       "l2": (f"inputs fit in L2 ({N * n * 4 / 1e6:.0f} MB patch matrix): L2 flushed before "
+                              f"each step by a {2 * l2_bytes / 1e6:.0f} MB write, steps timed one by one"
+                              if fits_l2 else
+                              f"inputs larger than L2 ({N * n * 4 / 1e6:.0f} MB patch matrix), no flush"),
                        "parallelism": f"replicas x{world}"},
             "e2e": {"value": e2e_value, "unit": "patches/s", "h2d_bytes_per_step": int(W * H * 4),
                     "d2h_bytes_per_step": int(W * H * 4), "ms_per_call": e2e_call_ms,
