@@ -111,3 +111,42 @@ def test_uneven_images_vs_fp64_oracle(torch_cuda, ksvd, oracle, synth, side, pw,
     assert np.all(np.isfinite(out))
     pg, pr = synth.psnr(clean, out), synth.psnr(clean, ref)
     assert abs(pg - pr) <= 0.05, (pg, pr)
+
+
+def test_update_mixed_atom_sizes_deterministic(torch_cuda, ksvd, oracle, synth):
+    """16x16 patches of an image that is flat outside a textured cross: three
+    atoms carry more than 13,000 entries beside small ones; the largest has
+    more than the sweep's CTAs hold in shared memory, so part of its columns
+    stream from the residual on every pass.  Atoms and coefficients against
+    the FP64 oracle (1e-4); two runs agree bit for bit."""
+    S, K, L = 224, 32, 3
+    tex = synth.add_gaussian(synth.clean_image(S, 70), 10.0, 70)
+    img = np.full((S, S), 100.0, np.float32)
+    img[88:136, :] = tex[88:136, :]
+    img[:, 88:136] = tex[:, 88:136]
+    Y = oracle.extract_patches(img, 16, 16, 1, 1)
+    D = oracle.init_dictionary(Y, K, int_norm=True, dtype=np.float32)
+    idx, coef = oracle.omp(Y, D, L, dtype=np.float32)
+    cnt = np.bincount(idx[(idx >= 0) & (coef != 0)], minlength=K)
+    assert (cnt > 13100).sum() >= 2 and (cnt < 5000).sum() >= 10, cnt
+    c = mkctx(ksvd, patch_width_dim=16, patch_height_dim=16, sliding_width=1, sliding_height=1, atoms=K,
+              omp_iter=L, compat=1)
+    Yd, idd = dev(torch_cuda, Y), dev(torch_cuda, idx)
+    runs = []
+    for _ in range(2):
+        Dd, cd = dev(torch_cuda, D), dev(torch_cuda, coef.astype(np.float32))
+        c.profile(1)
+        c.profile_reset()
+        c.update_dictionary(Yd, Dd, idd, cd)
+        torch_cuda.cuda.synchronize()
+        cn = c.profile_counters()
+        c.profile(0)
+        runs.append((Dd.cpu().numpy(), cd.cpu().numpy()))
+        assert cn["atoms_updated"] == K
+    np.testing.assert_array_equal(runs[0][0], runs[1][0])
+    np.testing.assert_array_equal(runs[0][1], runs[1][1])
+    Dr, cr = oracle.update_dictionary(Y.astype(np.float64), D.astype(np.float64), idx, coef.astype(np.float64),
+                                      q1_cap=False)
+    err = np.abs(runs[0][0] - Dr).max()
+    assert err < 1e-4, err
+    assert np.abs(runs[0][1] - cr).max() < 1e-4 * np.abs(cr).max()
