@@ -409,6 +409,30 @@ def main():
                 traffic = None
         achieved = bytes_per_patch * N / (avg_ms / 1000.0) / 1e9
         peak = float(peaks.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"]))
+        peak_tc = float(peaks.get("bf16_tflops", PEAKS_FALLBACK["bf16_tflops"]))
+        # every kernel family against its own bound (algorithmic work per
+        # patch x patches / device time per step); the correlation of the
+        # 16-bit forms against the tensor peak, the rest against HBM
+        flops_pp = 2 * n * K * L
+        per_kernel = {}
+        for f, bpp in (("omp", 4 * n + 8 * L), ("update", L * (4 * n + 8) + 4 * L), ("residual", 8 * n + 8 * L),
+                       ("csr", 12 * L)):
+            ms_f = fam[f][0] / max(args.steps, 1)
+            if ms_f <= 0:
+                continue
+            gbs = bpp * N / (ms_f / 1000.0) / 1e9
+            per_kernel[f] = {"ms_per_step": ms_f, "bytes_per_patch": bpp, "achieved_gbs": gbs,
+                             "frac_hbm": gbs / peak}
+            if f == "omp" and args.precision != "fp32":
+                tfs = flops_pp * N / (ms_f / 1000.0) / 1e12
+                per_kernel[f].update({"flops_per_patch": flops_pp, "achieved_tflops": tfs,
+                                      "frac_tensor": tfs / peak_tc})
+        # the whole iteration against max(F / tensor peak, B / HBM peak) with
+        # the compulsory bytes B = 4n + 8L (OMP) + L(4n + 8) + 4L (update)
+        b_iter = 4 * n + 8 * L + L * (4 * n + 8) + 4 * L
+        t_bound = max(flops_pp * N / (peak_tc * 1e12), b_iter * N / (peak * 1e9))
+        iter_bound = {"bytes_per_patch": b_iter, "flops_per_patch": flops_pp,
+                      "bound_patches_per_s": N / t_bound, "frac": (value / world) / (N / t_bound)}
         cpu = None
         if not args.no_cpu_baseline:
             oracle = load_oracle()
@@ -435,6 +459,8 @@ def main():
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
                          "algorithmic_bytes_per_patch": bytes_per_patch, "avg_launch_ms": avg_ms},
             "kernel_ms_per_step": {f: fam[f][0] / max(args.steps, 1) for f in fam},
+            "roofline_per_kernel": per_kernel,
+            "iteration_vs_bound": iter_bound,
             "phase_ms_one_step": {
                 name: phases[i] for i, name in (
                     (7, "upd_setup"), (0, "upd_wait_prev_atom"), (1, "upd_load"), (2, "upd_pass"),
