@@ -166,6 +166,12 @@ KSVD_DEV void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
 }
 
 // 1-D bulk copy; dst, src 16-byte aligned, bytes a multiple of 16.
+// Hint: bring [src, src + bytes) into L2 (16-byte aligned, a multiple of 16
+// bytes, inside an allocation).
+KSVD_DEV void bulk_prefetch_l2(const void* src, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 KSVD_DEV void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
   asm volatile(
       "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),

@@ -315,29 +315,52 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       const int p = t / n, k = t - p * n;
       Ys[p * ysn + k] = (p < np) ? __ldg(Y + p0 * n + t) : 0.0f;
     }
+    if (tid == 0 && tile + gridDim.x < ntiles) {
+      // this CTA's next tile of patches into L2 while this one is worked on
+      const int64_t pn = p0 + int64_t(gridDim.x) * kTcTile;
+      const int64_t np_next = (N - pn < kTcTile) ? N - pn : kTcTile;
+      const float* src = Y + pn * n;
+      const unsigned bytes = unsigned(np_next * n * 4) & ~15u;
+      if ((reinterpret_cast<uintptr_t>(src) & 15) == 0 && bytes > 0) bulk_prefetch_l2(src, bytes);
+    }
     __syncthreads();
-    // per-patch sums (quarter 0 thread), then the first A operand row
-    if (q == 0) {
+    // per-patch sums, a quarter of the features per thread (combined in a
+    // fixed order), then the first A operand row
+    {
       float ys = 0.0f;
       double yy = 0.0;
-      for (int k = 0; k < n; ++k) {
+      for (int k = q; k < n; k += kTcQ) {
         ys += yr[k];
         yy = fma(double(yr[k]), double(yr[k]), yy);
       }
+      X.part[q].x = ys;
+      X.qmask[q] = static_cast<unsigned long long>(__double_as_longlong(yy));
+    }
+    __syncthreads();
+    {
+      const float ys = (X.part[0].x + X.part[1].x) + (X.part[2].x + X.part[3].x);
       const float mean = ys / float(n);
       float mx = 0.0f, cc = 0.0f;
-      for (int k = 0; k < n; ++k) {
+      for (int k = q; k < n; k += kTcQ) {
         const float c = yr[k] - mean;
         mx = fmaxf(mx, fabsf(c));
         cc = fmaf(c, c, cc);
       }
-      P.cnt = 0;
-      P.done = m >= np;
-      P.ysum = ys;
-      P.yy = yy;
-      P.rmean = mean;
-      P.rscale = pow2_scale(mx);
-      P.rnorm = sqrtf(cc);
+      __syncthreads();  // every quarter has read the sums
+      X.part[q] = make_float2(mx, cc);
+      __syncthreads();
+      if (q == 0) {
+        double yy = 0.0;
+#pragma unroll
+        for (int j = 0; j < kTcQ; ++j) yy += __longlong_as_double(static_cast<long long>(X.qmask[j]));
+        P.cnt = 0;
+        P.done = m >= np;
+        P.ysum = ys;
+        P.yy = yy;
+        P.rmean = mean;
+        P.rscale = pow2_scale(fmaxf(fmaxf(X.part[0].x, X.part[1].x), fmaxf(X.part[2].x, X.part[3].x)));
+        P.rnorm = sqrtf((X.part[0].y + X.part[1].y) + (X.part[2].y + X.part[3].y));
+      }
     }
     __syncthreads();
     {
