@@ -393,7 +393,7 @@ def main():
         dom = max(("omp", "update"), key=lambda f: fam[f][0])
         dom_ms, dom_launches = fam[dom]
         avg_ms = dom_ms / max(dom_launches, 1)
-        # algorithmic bytes per launch (per patch figures):
+        # algorithmic bytes per launch, per patch times the patches of a launch:
         #   omp: read the patch (4n) + write the codes (8L)
         #   update: read the patch once per used atom + code (L(4n+8)) + write coefficients (4L)
         if dom == "omp":
