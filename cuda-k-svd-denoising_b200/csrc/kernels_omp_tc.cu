@@ -577,33 +577,28 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           } else {
             Lat(k, k) = sqrt(piv2);
             Ss[m * L + k] = a;
-            bv[m * L + k] = bbb;
+            // bv holds the forward solution z = L^-1 b of the support so far;
+            // only its new element is computed
+            double zk = bbb;
+            for (int j = 0; j < k; ++j) zk -= Lat(k, j) * bv[m * L + j];
+            zk /= Lat(k, k);
+            bv[m * L + k] = zk;
             double yv[kTcLMax];
-            for (int i = 0; i <= k; ++i) {
-              double s3 = bv[m * L + i];
-              for (int j = 0; j < i; ++j) s3 -= Lat(i, j) * yv[j];
-              yv[i] = s3 / Lat(i, i);
-            }
             for (int i = k; i >= 0; --i) {
-              double s3 = yv[i];
+              double s3 = bv[m * L + i];
               for (int j = i + 1; j <= k; ++j) s3 -= Lat(j, i) * yv[j];
               yv[i] = s3 / Lat(i, i);
             }
             for (int i = 0; i <= k; ++i) gam[m * L + i] = float(yv[i]);
             const int kk = k + 1;
             P.cnt = kk;
-            // |r|^2 = |y|^2 - 2 g.b + |L^T g|^2 bounds |r - rmean|; mean of
-            // r from the patch sum and the atom sums
+            // |r|^2 = |y|^2 - |L^-1 b|^2 (least squares) bounds |r - rmean|;
+            // mean of r from the patch sum and the atom sums
             double rr = P.yy;
             float rs = P.ysum;
             for (int i = 0; i < kk; ++i) {
-              rr -= 2.0 * double(gam[m * L + i]) * bv[m * L + i];
+              rr -= bv[m * L + i] * bv[m * L + i];
               rs = fmaf(-gam[m * L + i], asum[Ss[m * L + i]], rs);
-            }
-            for (int j = 0; j < kk; ++j) {
-              double z = 0.0;
-              for (int i = j; i < kk; ++i) z += Lat(i, j) * double(gam[m * L + i]);
-              rr += z * z;
             }
             P.rmean = rs / float(n);
             P.rscale = pow2_scale(float(sqrt(fmax(rr, 0.0))) * 1.01f + 1e-30f);
