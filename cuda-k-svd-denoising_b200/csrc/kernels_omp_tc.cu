@@ -567,7 +567,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           for (int i = 0; i < k; ++i) {
             double s3 = Gram[int64_t(Ss[m * L + i]) * K + a];
             for (int j = 0; j < i; ++j) s3 -= Lat(i, j) * Lat(k, j);
-            const double wi = s3 / Lat(i, i);
+            const double wi = s3 * Lat(i, i);  // the diagonal is kept as 1 / L_ii
             Lat(k, i) = wi;
             ww += wi * wi;
           }
@@ -575,19 +575,19 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           if (!(piv2 > 0.0)) {
             stop = true;  // the new atom depends linearly on the support
           } else {
-            Lat(k, k) = sqrt(piv2);
+            Lat(k, k) = 1.0 / sqrt(piv2);
             Ss[m * L + k] = a;
             // bv holds the forward solution z = L^-1 b of the support so far;
             // only its new element is computed
             double zk = bbb;
             for (int j = 0; j < k; ++j) zk -= Lat(k, j) * bv[m * L + j];
-            zk /= Lat(k, k);
+            zk *= Lat(k, k);
             bv[m * L + k] = zk;
             double yv[kTcLMax];
             for (int i = k; i >= 0; --i) {
               double s3 = bv[m * L + i];
               for (int j = i + 1; j <= k; ++j) s3 -= Lat(j, i) * yv[j];
-              yv[i] = s3 / Lat(i, i);
+              yv[i] = s3 * Lat(i, i);
             }
             for (int i = 0; i <= k; ++i) gam[m * L + i] = float(yv[i]);
             const int kk = k + 1;
