@@ -275,11 +275,22 @@ bool Sm100KSvdDenoiser::internalDenoising() {
     lastError = std::string("ksvd_create: ") + ksvd_status_string(st);
     return false;
   }
-  output.width = input.width;
-  output.height = input.height;
-  output.data.assign(input.data.size(), 0.0f);
-  st = ksvd_denoise(ctx, input.data.data(), input.width, input.height, sigma, output.data.data(), &stats_);
+  // The reference transposes the loaded image and hands its column-major
+  // matrix on (denoiser.cpp:46-51); its patch walk, dictionary seeds and
+  // sub-images therefore follow the image's columns.  The library gets the
+  // same buffer, this image transposed as a row-major image, and the result
+  // is transposed back.
+  const int W = input.width, H = input.height;
+  std::vector<float> tin(size_t(W) * H), tout(size_t(W) * H, 0.0f);
+  for (int y = 0; y < H; ++y)
+    for (int x = 0; x < W; ++x) tin[size_t(x) * H + y] = input.data[size_t(y) * W + x];
+  st = ksvd_denoise(ctx, tin.data(), H, W, sigma, tout.data(), &stats_);
   if (st != KSVD_OK) lastError = ksvd_last_error(ctx);
+  output.width = W;
+  output.height = H;
+  output.data.assign(size_t(W) * H, 0.0f);
+  for (int y = 0; y < H; ++y)
+    for (int x = 0; x < W; ++x) output.data[size_t(y) * W + x] = tout[size_t(x) * H + y];
   ksvd_destroy(ctx);
   timeElapsed.working = ms_between(t0, clk::now());
   return st == KSVD_OK;

@@ -273,20 +273,29 @@ def test_speckle_roundtrip(oracle, synth):
     assert np.all(np.isfinite(out)) and out.min() > 0
 
 
-def test_golden_fixtures(oracle):
-    """Fixtures in tests/golden/ (see tests/golden/README.md) replayed on the
-    FP32 oracle."""
+def test_reference_outputs_psnr(oracle, synth):
+    """The reference's own stored GPU results (tests/golden/
+    reference_barbara_psnr.npz, made by make_reference_psnr.py from the
+    reference's test images): barbara 160 x 160 at three noise levels, 256
+    atoms, after 1, 5 and 10 K-SVD iterations, with the settings of the
+    reference's config.json (8 x 8 patches, stride 2, 5 OMP atoms).  The FP32
+    oracle, given the image transposed as the reference's loader hands it on
+    (denoiser.cpp:46-51), must land within 0.6 dB PSNR of each stored result.
+    A loose pin: the reference estimated sigma^2 with CImg's variance_noise,
+    which is not available here; the oracle gets the empirical noise variance
+    (the clean image is known)."""
     from pathlib import Path
-    gdir = Path(__file__).parent / "golden"
-    files = sorted(gdir.glob("*.npz"))
-    if not files:
-        pytest.skip("no golden fixtures committed")
-    for f in files:
-        z = np.load(f)
-        kind = str(z["kind"])
-        if kind == "omp":
-            idx, coef = oracle.omp(z["patches"], z["dict"], int(z["L"]), dtype=np.float32)
-            agree = np.mean(np.all(idx == z["idx"], axis=1))
-            assert agree >= float(z["min_agree"]), (f.name, agree)
-            m = np.all(idx == z["idx"], axis=1)
-            np.testing.assert_allclose(coef[m], z["coef"][m], rtol=float(z["rtol"]), atol=float(z["atol"]))
+    z = np.load(Path(__file__).parent / "golden" / "reference_barbara_psnr.npz")
+    assert str(z["kind"]) == "reference_psnr"
+    clean = z["clean"].astype(np.float32)
+    p, s = int(z["patch"]), int(z["stride"])
+    for li in range(len(z["levels"])):
+        noisy = z["noisy"][li].astype(np.float32)
+        sigma2 = float(np.var(noisy - clean))
+        for ii, it in enumerate(z["iters"]):
+            out, _ = oracle.ksvd_denoise(np.ascontiguousarray(noisy.T), sigma2, pw=p, ph=p, sw=s, sh=s,
+                                         atoms=int(z["atoms"]), ksvd_iter=int(it), omp_iter=int(z["omp_iter"]),
+                                         q1_cap=True, int_norm=True, dtype=np.float32)
+            got = synth.psnr(clean, np.clip(np.round(out.T), 0, 255))
+            ref = float(z["ref_psnr"][li, ii])
+            assert abs(got - ref) <= 0.6, (str(z["levels"][li]), int(it), got, ref)
