@@ -5,11 +5,13 @@
 // path, by bench.py as the timed CPU baseline ("port"), and nowhere else:
 // the product library never links or calls it.
 //
-// Parity unpinned: the reference ships no golden vectors for this path and
-// its own GPU code could not be run to make some (its denoiser layer needs
-// the absent CImg library; its OMP layer aborted with an illegal address on
-// a B200).  The restatement is checked against independent numpy / LAPACK
-// restatements of each step instead.
+// Parity unpinned at the level of supports, coefficients and atoms: the
+// reference ships no golden vectors for this path and its own GPU code could
+// not be run to make some (its denoiser layer needs the absent CImg library;
+// its OMP layer aborted with an illegal address on a B200).  The restatement
+// is checked against independent numpy / LAPACK restatements of each step,
+// and loosely (PSNR within 0.6 dB) against the reference's stored GPU
+// results for its barbara test images (tests/golden/).
 //
 // Every function names the reference lines it follows.  The scalar type T is
 // double for the FP64 oracle and float for the FP32 restatement; the tiny
