@@ -150,7 +150,10 @@ ksvd_status validate_params(const ksvd_params* p, std::string* why) {
 }
 
 ksvd_status check_kernel_support(ksvd_ctx* c) {
-  const int n = c->p.patch_width_dim * c->p.patch_height_dim, K = c->p.atoms, L = c->p.omp_iter;
+  // the patch area is bounded before it is formed as an int
+  const int64_t n64 = int64_t(c->p.patch_width_dim) * c->p.patch_height_dim;
+  if (n64 < 1 || n64 > 512) return fail(c, KSVD_ERR_INVALID, "patch size pw x ph must be in [1, 512]");
+  const int n = int(n64), K = c->p.atoms, L = c->p.omp_iter;
   if (!ksvd::omp_tc_supported(n, K, L) && !ksvd::omp_fp32_supported(n, K, L) && !ksvd::omp_stream_supported(n, K, L))
     return fail(c, KSVD_ERR_INVALID, "patch size x atoms x ompIter beyond every OMP kernel (atoms <= 1024)");
   if (!ksvd::update_res_supported(n))
@@ -376,7 +379,9 @@ ksvd_status ksvd_extract_patches(ksvd_ctx* c, const float* d_img, int width, int
 ksvd_status ksvd_init_dictionary(ksvd_ctx* c, const float* d_patches, int64_t N, float* d_dict) {
   KSVD_TRY(check_ctx(c));
   if (!d_patches || !d_dict) return fail(c, KSVD_ERR_INVALID, "null pointer");
-  const int n = c->p.patch_width_dim * c->p.patch_height_dim, K = c->p.atoms;
+  const int64_t n64 = int64_t(c->p.patch_width_dim) * c->p.patch_height_dim;
+  if (n64 < 1 || n64 > (int64_t(1) << 20)) return fail(c, KSVD_ERR_INVALID, "patch area out of range");
+  const int n = int(n64), K = c->p.atoms;
   if (N < 1 || N / 2 + K > N) return fail(c, KSVD_ERR_INVALID, "fewer patches than N/2 + atoms");
   {
     Prof pr(c, "init_dict", 1);

@@ -10,6 +10,7 @@ namespace ksvd {
 bool make_geom(int W, int H, int pw, int ph, int sw, int sh, PatchGeom* g) {
   if (W <= 0 || H <= 0 || pw <= 0 || ph <= 0 || sw <= 0 || sh <= 0) return false;
   if (ph > W || pw > H) return false;
+  if (int64_t(pw) * ph > (int64_t(1) << 20)) return false;  // the patch area must fit an int comfortably
   g->W = W;
   g->H = H;
   g->pw = pw;

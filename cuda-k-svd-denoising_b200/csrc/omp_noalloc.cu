@@ -70,8 +70,11 @@ ksvd_status gram_scratch(int device, double** out) {
 extern "C" ksvd_status ksvd_omp_noalloc(const ksvd_params* p, const float* d_patches, int64_t num_patches,
                                         const float* d_dict, int32_t* d_idx, float* d_coef, void* stream) {
   if (!p || !d_patches || !d_dict || !d_idx || !d_coef || num_patches < 1) return KSVD_ERR_INVALID;
-  const int n = p->patch_width_dim * p->patch_height_dim, K = p->atoms, L = p->omp_iter;
-  if (p->patch_width_dim < 1 || p->patch_height_dim < 1 || K < 1 || L < 1 || L > 32) return KSVD_ERR_INVALID;
+  if (p->patch_width_dim < 1 || p->patch_height_dim < 1) return KSVD_ERR_INVALID;
+  const int64_t n64 = int64_t(p->patch_width_dim) * p->patch_height_dim;  // bounded before it becomes an int
+  if (n64 > (int64_t(1) << 20)) return KSVD_ERR_INVALID;
+  const int n = int(n64), K = p->atoms, L = p->omp_iter;
+  if (K < 1 || L < 1 || L > 32) return KSVD_ERR_INVALID;
   if (K > kNoAllocMaxAtoms) return KSVD_ERR_TOO_LARGE;
   if (!ksvd::omp_fp32_supported(n, K, L)) return KSVD_ERR_INVALID;
   int device = 0;

@@ -75,3 +75,13 @@ def test_create_without_gpu_reports_no_device(ksvd, built_lib):
 def test_null_context_is_rejected(built_lib, ksvd):
     assert built_lib.ksvd_omp(None, None, 0, None, None, None) == ksvd.ERR_INVALID
     assert built_lib.ksvd_last_error(None) == b"null context"
+
+
+def test_noalloc_rejects_patch_areas_that_do_not_fit_an_int(ksvd, built_lib):
+    """4 x (2^30 + 36) would wrap to 144 as a 32-bit product: rejected before
+    any device work (the pointers are never touched)."""
+    fake = ctypes.c_void_p(16)
+    for pw, ph in ((4, 2 ** 30 + 36), (2 ** 16, 2 ** 16), (0, 8), (8, -1)):
+        p = ksvd.make_params(patch_width_dim=pw, patch_height_dim=ph)
+        st = built_lib.ksvd_omp_noalloc(ctypes.byref(p), fake, ctypes.c_int64(1000), fake, fake, fake, None)
+        assert st == ksvd.ERR_INVALID, (pw, ph, st)
