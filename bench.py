@@ -184,6 +184,54 @@ def cpu_baseline(pkg, oracle, wl, budget_s=40.0):
                       f"{what} of the workload's {N} patches, {dt:.1f} s"}, dt
 
 
+def quality_vs_fp64(pkg, oracle, wl, clean, noisy, D0, patches, make_ctx, forms):
+    """Accuracy of every form against the FP64 oracle on this workload (the
+    checker, run after all timed regions): support agreement and coefficient
+    error of the first OMP call from the shared initial dictionary, atom and
+    coefficient error of the first update sweep from the FP64 codes, and the
+    PSNR of the whole denoise beside the FP64 oracle's.  The oracle runs the
+    same update mode as the timed steps (no 1024-patch cap)."""
+    import torch
+    import quality as q
+    t0 = time.perf_counter()
+    ref = q.fp64_reference(oracle, noisy, D0, patch=wl.patch, stride=wl.stride, omp_iter=wl.omp_iter,
+                           ksvd_iter=wl.ksvd_iter, q1_cap=False, sigma2=wl.sigma ** 2)
+    t_ref = time.perf_counter() - t0
+    psnr64 = pkg.synth.psnr(clean, ref["image"])
+    N, L = patches.shape[0], wl.omp_iter
+    Dd = torch.from_numpy(D0).cuda()
+    torch.cuda.synchronize()  # the contexts run on their own stream
+    res = {"fp64_oracle_psnr": psnr64, "fp64_oracle_seconds": t_ref, "oracle_threads": oracle.max_threads(),
+           "forms": {}}
+    for form in forms:
+        c, _ = make_ctx(form)
+        idx = torch.empty((N, L), dtype=torch.int32, device="cuda")
+        coef = torch.empty((N, L), dtype=torch.float32, device="cuda")
+        c.omp(patches, Dd, idx, coef)
+        torch.cuda.synchronize()
+        i, cf = idx.cpu().numpy(), coef.cpu().numpy()
+        out, _ = c.denoise(noisy, wl.sigma ** 2)
+        p = pkg.synth.psnr(clean, out)
+        res["forms"][form] = {"support_agreement": q.support_agreement(i, ref["idx0"]),
+                              "coef_rel_err": q.coef_rel_err(i, cf, ref["idx0"], ref["coef0"]),
+                              "psnr": p, "dpsnr_vs_fp64": p - psnr64}
+        c.close()
+    # the update sweep is shared by every form
+    c, _ = make_ctx("fp32")
+    D1 = torch.from_numpy(D0.copy()).cuda()
+    idx = torch.from_numpy(ref["idx0"]).cuda()
+    coef = torch.from_numpy(ref["coef0"].astype(np.float32)).cuda()
+    torch.cuda.synchronize()
+    c.update_dictionary(patches, D1, idx, coef)
+    torch.cuda.synchronize()
+    res["update_atom_err"] = q.atom_err(D1.cpu().numpy(), ref["D1"])
+    res["update_coef_rel_err"] = q.coef_rel_err(ref["idx0"], coef.cpu().numpy(), ref["idx0"], ref["coef1"])
+    c.close()
+    res["bars"] = {"support_agreement": ">= 0.999", "coef_rel_err": "<= 1e-4", "update_atom_err": "<= 1e-4",
+                   "dpsnr_vs_fp64": "|.| <= 0.05 dB"}
+    return res
+
+
 def run_reference(args, wl):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -233,13 +281,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="img2048_p12s3_k256")
-    ap.add_argument("--precision", default="fp16", choices=["fp32", "bf16", "fp16"],
+    ap.add_argument("--precision", default="fp16", choices=["fp32", "bf16", "fp16", "learned"],
                     help="headline form; the other forms are timed beside it unless --no-forms")
     ap.add_argument("--no-forms", action="store_true")
     ap.add_argument("--compat", type=int, default=1, help="KSVD_COMPAT_* bits (1 = INT_NORM, 3 = +Q1 cap)")
     ap.add_argument("--e2e-calls", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=40.0)
+    ap.add_argument("--no-quality", action="store_true",
+                    help="skip the accuracy report against the FP64 oracle (about a minute of CPU)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -258,7 +308,9 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
 
     ksvd = pkg.ksvd
-    precs = {"fp32": ksvd.PREC_FP32, "bf16": ksvd.PREC_BF16_RESCORE, "fp16": ksvd.PREC_FP16_RESCORE}
+    precs = {"fp32": ksvd.PREC_FP32, "bf16": ksvd.PREC_BF16_RESCORE, "fp16": ksvd.PREC_FP16_RESCORE,
+             "learned": ksvd.PREC_BF16_LEARNED}
+    learned = {}  # the fitted proposal (parameters, fit statistics), shared by the learned contexts
 
     def make_ctx(form):
         params = ksvd.make_params(patch_width_dim=wl.patch, patch_height_dim=wl.patch, sliding_width=wl.stride,
@@ -266,10 +318,20 @@ def main():
                                   ksvd_iter=wl.ksvd_iter, precision=precs[form], compat=args.compat, device=local)
         c = ksvd.Context(params)
         c.set_stream(stream.cuda_stream)
+        if form == "learned":
+            c.set_noise_variance(wl.sigma ** 2)
+            if "params" in learned:
+                c.proposal_set_params(learned["params"])
+            else:
+                # supports of ksvd_iter - 1 plain FP32 iterations from the
+                # initial dictionary (about N x 9 pairs), 2 epochs
+                st = c.proposal_fit(patches, D0, iters=max(1, wl.ksvd_iter - 1), epochs=2, seed=wl.seed)
+                learned["params"] = c.proposal_get_params()
+                learned["fit"] = st
         return c, params
 
     stream = torch.cuda.Stream()
-    ctx, params = make_ctx(args.precision)
+    ctx, params = make_ctx("fp32" if args.precision == "learned" else args.precision)
 
     # each rank: its own seeded image (replicas)
     wlr = replica_workload(wl, rank)
@@ -289,6 +351,9 @@ def main():
     ctx.extract_patches(img_d, patches)
     ctx.init_dictionary(patches, D)
     D0 = D.clone()
+    if args.precision == "learned":
+        ctx.close()
+        ctx, params = make_ctx("learned")
     # the step's working set is the patch matrix plus the residual matrix of
     # the same size; below the L2 size (126 MB) steps are timed one by one
     # with an L2 flush between them
@@ -342,7 +407,8 @@ def main():
         if dist:
             dist.barrier()
         ms = sum(e0.elapsed_time(e1) for e0, e1 in evs) / args.steps
-        fams = {f: c.profile_read(f) for f in ("gram", "omp", "csr", "residual", "update")}
+        fams = {f: c.profile_read(f) for f in ("gram", "omp", "csr", "residual", "update", "proposal",
+                                                "omp_restricted", "omp_fallback")}
         cn = c.profile_counters()
         # one more (untimed) iteration with the in-kernel phase timers on
         c.profile_reset()
@@ -358,13 +424,18 @@ def main():
     ms_step, fam, phases, counters, gpu_launches, clk_summary = timed_steps(ctx, True)
     value = aggregate_rate(N, world, ms_step)
     forms = {args.precision: value}
+    fallback_rate = None
+    if args.precision == "learned":
+        fallback_rate = ctx.proposal_fallbacks()["last"] / N
     if not args.no_forms:
-        for form in ("fp32", "fp16", "bf16"):
+        for form in ("fp32", "fp16", "bf16", "learned"):
             if form == args.precision:
                 continue
             c2, _ = make_ctx(form)
             ms2 = timed_steps(c2, False)[0]
             forms[form] = aggregate_rate(N, world, ms2)
+            if form == "learned":
+                fallback_rate = c2.proposal_fallbacks()["last"] / N
             c2.close()
 
     # ---- e2e through the C ABI with pinned host buffers --------------------
@@ -437,11 +508,28 @@ def main():
         if not args.no_cpu_baseline:
             oracle = load_oracle()
             cpu, _ = cpu_baseline(pkg, oracle, wl, budget_s=args.cpu_budget)
+        acc = None
+        if not args.no_quality and world == 1:
+            acc = quality_vs_fp64(pkg, load_oracle(), wl, clean, noisy, D0.cpu().numpy(), patches, make_ctx,
+                                  list(forms))
+        # the metric by form: patches/s per iteration, ratio over the plain
+        # FP32 form, and the accuracy beside it
+        by_form = {}
+        for f, v in forms.items():
+            by_form[f] = {"patches_per_s": v, "ratio_vs_fp32": (v / forms["fp32"]) if "fp32" in forms else None}
+            if acc:
+                by_form[f].update(acc["forms"][f])
+        if "learned" in by_form:
+            by_form["learned"]["fallback_rate_last_step"] = fallback_rate
+            by_form["learned"]["fit"] = learned.get("fit")
+            by_form["learned"]["note"] = ("proposal fitted before timing on this image's own plain-FP32 supports "
+                                          "(ksvd_iter - 1 iterations, 2 epochs); fit time not in the metric")
         line = {
             "metric": "patches/s per K-SVD iteration", "value": value, "unit": "patches/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": {"fp32": "f32", "bf16": "bf16+f32+f64", "fp16": "f16+f32+f64"}[args.precision],
+            "dtype": {"fp32": "f32", "bf16": "bf16+f32+f64", "fp16": "f16+f32+f64",
+                      "learned": "bf16+f32+f64"}[args.precision],
             "data": "synthetic",
             "config": {"workload": wl.name, "image": f"{wl.size}x{wl.size}", "sigma": wl.sigma,
                        "patch": f"{wl.patch}x{wl.patch}", "stride": wl.stride, "num_patches": N, "atoms": K,
@@ -469,8 +557,10 @@ def main():
             "counters_per_step": {k: (v if k.startswith("omp_") else v / max(args.steps, 1))
                                   for k, v in counters.items()},
             "quality": {"psnr_noisy": psnr_noisy, "psnr_denoised": psnr_out,
-                        "power_iters_last_sweep": st.power_iters, "atoms_updated_last_sweep": st.atoms_updated},
+                        "power_iters_last_sweep": st.power_iters, "atoms_updated_last_sweep": st.atoms_updated,
+                        "vs_fp64_oracle": acc},
             "forms_patches_per_s": forms,
+            "metric_by_form": by_form,
             "clocks": clk_summary,
         }
         if cpu:

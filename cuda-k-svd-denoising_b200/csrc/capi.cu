@@ -8,124 +8,14 @@
 #include <new>
 #include <string>
 
+#include "capi_common.cuh"
 #include "ksvd_internal.cuh"
 
 using ksvd::PatchGeom;
 
 namespace {
 
-ksvd_status fail(ksvd_ctx* c, ksvd_status st, const std::string& msg) {
-  if (c) c->err = msg;
-  return st;
-}
-
-ksvd_status cuda_fail(ksvd_ctx* c, cudaError_t e, const char* what) {
-  std::string m = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
-  if (e == cudaErrorMemoryAllocation) return fail(c, KSVD_ERR_NO_MEMORY, m);
-  return fail(c, KSVD_ERR_CUDA, m);
-}
-
-#define KSVD_CU(ctx, expr, what)                      \
-  do {                                                \
-    cudaError_t e_ = (expr);                          \
-    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, what); \
-  } while (0)
-
-#define KSVD_TRY(expr)                 \
-  do {                                 \
-    ksvd_status s_ = (expr);           \
-    if (s_ != KSVD_OK) return s_;      \
-  } while (0)
-
-// Named device buffer that only grows.
-ksvd_status ws(ksvd_ctx* c, const char* name, size_t bytes, void** out) {
-  auto& b = c->bufs[name];
-  if (bytes == 0) bytes = 16;
-  if (b.bytes < bytes) {
-    if (b.ptr) cudaFree(b.ptr);
-    b.ptr = nullptr;
-    b.bytes = 0;
-    cudaError_t e = cudaMalloc(&b.ptr, bytes);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      return cuda_fail(c, e, (std::string("allocating ") + name).c_str());
-    }
-    b.bytes = bytes;
-  }
-  *out = b.ptr;
-  return KSVD_OK;
-}
-
-template <typename T>
-ksvd_status wsT(ksvd_ctx* c, const char* name, size_t count, T** out) {
-  void* p = nullptr;
-  KSVD_TRY(ws(c, name, count * sizeof(T), &p));
-  *out = static_cast<T*>(p);
-  return KSVD_OK;
-}
-
-cudaEvent_t get_event(ksvd_ctx* c) {
-  if (!c->event_pool.empty()) {
-    cudaEvent_t e = c->event_pool.back();
-    c->event_pool.pop_back();
-    return e;
-  }
-  cudaEvent_t e = nullptr;
-  cudaEventCreate(&e);
-  return e;
-}
-
-// Records CUDA events around the launches of one kernel family when
-// profiling is on; always counts launches.
-struct Prof {
-  ksvd_ctx* c;
-  ksvd_ctx::Family* f = nullptr;
-  cudaEvent_t e0 = nullptr;
-  int kernels;
-  Prof(ksvd_ctx* ctx, const char* fam, int nkernels) : c(ctx), kernels(nkernels) {
-    if (c->profiling) {
-      f = &c->families[fam];
-      e0 = get_event(c);
-      cudaEventRecord(e0, c->stream);
-    }
-  }
-  ~Prof() {
-    c->launch_count += kernels;
-    if (f) {
-      cudaEvent_t e1 = get_event(c);
-      cudaEventRecord(e1, c->stream);
-      f->pending.emplace_back(e0, e1);
-      f->launches += 1;
-    }
-  }
-};
-
-ksvd_status check_ctx(ksvd_ctx* c) {
-  if (!c) return KSVD_ERR_INVALID;
-  cudaError_t e = cudaSetDevice(c->device);
-  if (e != cudaSuccess) return cuda_fail(c, e, "cudaSetDevice");
-  return KSVD_OK;
-}
-
-// Reads and clears the device error word (synchronises the stream).
-ksvd_status check_dev_flags(ksvd_ctx* c, const char* where) {
-  ksvd::GridBarrier h{};
-  KSVD_CU(c, cudaMemcpyAsync(&h, c->d_flags, sizeof(h), cudaMemcpyDeviceToHost, c->stream), "reading flags");
-  KSVD_CU(c, cudaStreamSynchronize(c->stream), where);
-  if (h.err != ksvd::DEVERR_NONE) {
-    cudaMemsetAsync(c->d_flags, 0, sizeof(ksvd::GridBarrier), c->stream);
-    cudaStreamSynchronize(c->stream);
-    switch (h.err) {
-      case ksvd::DEVERR_TIMEOUT:
-        return fail(c, KSVD_ERR_TIMEOUT, std::string(where) + ": a bounded grid-barrier wait timed out");
-      case ksvd::DEVERR_ZERO_ATOM:
-        return fail(c, KSVD_ERR_NUMERIC, std::string(where) + ": an initial atom has zero norm");
-      default:
-        return fail(c, KSVD_ERR_CUDA, std::string(where) + ": device error flag set");
-    }
-  }
-  return KSVD_OK;
-}
+using namespace ksvd::api;
 
 bool geom_of(const ksvd_params& p, int W, int H, PatchGeom* g) {
   return ksvd::make_geom(W, H, p.patch_width_dim, p.patch_height_dim, p.sliding_width, p.sliding_height, g);
@@ -143,7 +33,7 @@ ksvd_status validate_params(const ksvd_params* p, std::string* why) {
   if (p->ksvd_iter < 0) return bad("ksvdIter must be >= 0");
   if (p->type < KSVD_CUDA_K_GESVD || p->type > KSVD_CUDA_K_SM100A) return bad("unknown type");
   if (p->precision != KSVD_PREC_FP32 && p->precision != KSVD_PREC_BF16_RESCORE &&
-      p->precision != KSVD_PREC_FP16_RESCORE)
+      p->precision != KSVD_PREC_FP16_RESCORE && p->precision != KSVD_PREC_BF16_LEARNED)
     return bad("unknown precision");
   if (p->sub_image_width_dim < 0 || p->sub_image_height_dim < 0) return bad("sub-image dimensions must be >= 0");
   return KSVD_OK;
@@ -393,8 +283,13 @@ ksvd_status ksvd_init_dictionary(ksvd_ctx* c, const float* d_patches, int64_t N,
   return check_dev_flags(c, "initDictionary");
 }
 
-static ksvd_status omp_impl(ksvd_ctx* c, const float* d_patches, int64_t N, const float* d_dict, int32_t* d_idx,
-                            float* d_coef) {
+}  // extern "C"
+
+namespace ksvd {
+namespace api {
+
+ksvd_status omp_form(ksvd_ctx* c, const float* d_patches, int64_t N, const float* d_dict, int32_t* d_idx,
+                     float* d_coef, int precision) {
   const int n = c->p.patch_width_dim * c->p.patch_height_dim, K = c->p.atoms, L = c->p.omp_iter;
   double* gram = nullptr;
   KSVD_TRY(wsT(c, "gram", size_t(K) * K, &gram));
@@ -402,15 +297,16 @@ static ksvd_status omp_impl(ksvd_ctx* c, const float* d_patches, int64_t N, cons
     Prof pr(c, "gram", 1);
     KSVD_CU(c, ksvd::launch_gram_f64(d_dict, K, n, gram, c->stream), "gram");
   }
+  if (precision == KSVD_PREC_BF16_LEARNED) return omp_learned_impl(c, d_patches, N, d_dict, gram, d_idx, d_coef);
   Prof pr(c, "omp", 1);
   ksvd::DevStats* ph = c->profiling >= 2 ? c->d_phase : nullptr;
   // The tensor-core forms need the 16-bit dictionary in shared memory (atoms
   // <= 256); beyond that, and for the FP32 form, the FP32 kernels run: the
   // resident-dictionary one when it fits, else the streamed one.
-  if (c->p.precision != KSVD_PREC_FP32 && ksvd::omp_tc_supported(n, K, L)) {
+  if (precision != KSVD_PREC_FP32 && ksvd::omp_tc_supported(n, K, L)) {
     KSVD_CU(c,
             ksvd::launch_omp_tc(d_patches, N, n, d_dict, gram, K, L, d_idx, d_coef, c->num_sms,
-                                c->p.precision == KSVD_PREC_FP16_RESCORE ? 1 : 0, c->d_flags, ph, c->stream),
+                                precision == KSVD_PREC_FP16_RESCORE ? 1 : 0, c->d_flags, ph, c->stream),
             "omp (tensor cores)");
   } else if (ksvd::omp_fp32_supported(n, K, L)) {
     KSVD_CU(c, ksvd::launch_omp_fp32(d_patches, N, n, d_dict, gram, K, L, d_idx, d_coef, c->num_sms, ph, c->stream),
@@ -423,6 +319,16 @@ static ksvd_status omp_impl(ksvd_ctx* c, const float* d_patches, int64_t N, cons
   return KSVD_OK;
 }
 
+}  // namespace api
+}  // namespace ksvd
+
+static ksvd_status omp_impl(ksvd_ctx* c, const float* d_patches, int64_t N, const float* d_dict, int32_t* d_idx,
+                            float* d_coef) {
+  return omp_form(c, d_patches, N, d_dict, d_idx, d_coef, c->p.precision);
+}
+
+extern "C" {
+
 ksvd_status ksvd_omp(ksvd_ctx* c, const float* d_patches, int64_t N, const float* d_dict, int32_t* d_idx,
                      float* d_coef) {
   KSVD_TRY(check_ctx(c));
@@ -432,8 +338,13 @@ ksvd_status ksvd_omp(ksvd_ctx* c, const float* d_patches, int64_t N, const float
   return check_dev_flags(c, "omp");
 }
 
-static ksvd_status update_impl(ksvd_ctx* c, const float* d_patches, int64_t N, float* d_dict, const int32_t* d_idx,
-                               float* d_coef) {
+}  // extern "C"
+
+namespace ksvd {
+namespace api {
+
+ksvd_status update_form(ksvd_ctx* c, const float* d_patches, int64_t N, float* d_dict, const int32_t* d_idx,
+                        float* d_coef) {
   const int n = c->p.patch_width_dim * c->p.patch_height_dim, K = c->p.atoms, L = c->p.omp_iter;
   ksvd::CsrWork w;
   w.nchunks = ksvd::csr_num_chunks(N);
@@ -448,13 +359,16 @@ static ksvd_status update_impl(ksvd_ctx* c, const float* d_patches, int64_t N, f
   KSVD_TRY(wsT(c, "upd_resid", size_t(N) * n, &resid));
   KSVD_TRY(wsT(c, "upd_partials", ksvd::update_res_partial_floats(n, grid), &gw));
   KSVD_TRY(wsT(c, "upd_sync", size_t(2) * K, &sync));
+  int* last = nullptr;
+  KSVD_TRY(wsT(c, "upd_last", size_t(N), &last));
   {
     Prof pr(c, "csr", 4);
     KSVD_CU(c, ksvd::launch_csr_build(d_idx, d_coef, N, L, K, w, c->stream), "csr build");
   }
   {
     Prof pr(c, "residual", 1);
-    KSVD_CU(c, ksvd::launch_residual(d_patches, N, n, d_dict, K, L, d_idx, d_coef, resid, c->num_sms, c->stream),
+    KSVD_CU(c,
+            ksvd::launch_residual(d_patches, N, n, d_dict, K, L, d_idx, d_coef, resid, last, c->num_sms, c->stream),
             "residual");
   }
   KSVD_CU(c, cudaMemsetAsync(c->d_stats, 0, sizeof(ksvd::DevStats), c->stream), "stats reset");
@@ -462,7 +376,7 @@ static ksvd_status update_impl(ksvd_ctx* c, const float* d_patches, int64_t N, f
   KSVD_CU(c,
           ksvd::launch_update_res(resid, n, d_dict, K, L, d_coef, w.atom_ptr, w.entries,
                                   (c->p.compat & KSVD_COMPAT_Q1_CAP) ? 1 : 0, gw, sync, c->d_flags, c->d_stats,
-                                  c->profiling >= 2 ? 1 : 0, grid, c->stream),
+                                  c->profiling >= 2 ? 1 : 0, last, c->upd_slice, grid, c->stream),
           "update");
   if (c->profiling) {
     // fold this sweep's phase timers into the profiling accumulator
@@ -470,6 +384,16 @@ static ksvd_status update_impl(ksvd_ctx* c, const float* d_patches, int64_t N, f
   }
   return KSVD_OK;
 }
+
+}  // namespace api
+}  // namespace ksvd
+
+static ksvd_status update_impl(ksvd_ctx* c, const float* d_patches, int64_t N, float* d_dict, const int32_t* d_idx,
+                               float* d_coef) {
+  return update_form(c, d_patches, N, d_dict, d_idx, d_coef);
+}
+
+extern "C" {
 
 ksvd_status ksvd_update_dictionary(ksvd_ctx* c, const float* d_patches, int64_t N, float* d_dict,
                                    const int32_t* d_idx, float* d_coef) {
@@ -585,6 +509,7 @@ ksvd_status ksvd_denoise(ksvd_ctx* c, const float* img, int width, int height, f
   if (width < 1 || height < 1) return fail(c, KSVD_ERR_INVALID, "empty image");
   if (!(sigma2 > 0.0f)) return fail(c, KSVD_ERR_INVALID, "sigma2 must be > 0");
   KSVD_TRY(check_kernel_support(c));
+  c->prop.sigma2 = sigma2;  // the learned OMP's fallback threshold
   const int tw = c->p.sub_image_width_dim, th = c->p.sub_image_height_dim;
   const bool tiled = tw != 0 || th != 0;
   if (tiled && (tw < 1 || th < 1 || th > width || tw > height))

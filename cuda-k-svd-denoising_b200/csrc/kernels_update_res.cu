@@ -15,7 +15,7 @@
 // with x_{j,p} = 0 (and r_p <- e_p) for entries beyond the cap.
 //
 // One persistent cooperative kernel walks the atoms.  An atom's entries are
-// split over `active` CTAs (about kUrTargetSlice entries each); each keeps its
+// split over `active` CTAs (about slice_target entries each); each keeps its
 // columns in shared memory (those beyond the capacity are re-read from the
 // residual on every pass).  A power step is one pass over the local columns
 // producing a partial w, then an all-reduce: each CTA writes its partial,
@@ -35,7 +35,7 @@ namespace ksvd {
 
 constexpr int kUrThreads = 512;
 constexpr int kUrWarps = kUrThreads / 32;
-constexpr int kUrTargetSlice = 64;    // entries per CTA before another CTA joins an atom
+constexpr int kUrDefaultSlice = 64;   // entries per CTA before another CTA joins an atom (default)
 constexpr int kUrMaxIters = 200;
 constexpr float kUrTol = 2.0e-7f;     // max |u_new - u_old| to stop
 constexpr size_t kUrSmemMax = 232448 - 256;  // opt-in shared memory per block, less the static part
@@ -48,22 +48,22 @@ __host__ __device__ inline int ur_n4(int n) { return (n + 3) & ~3; }
 __host__ __device__ inline int ur_es(int n) { return 4 * ((ur_n4(n) / 4) | 1); }
 constexpr int kUrRows = 32;  // reduction rows: 16 column groups + 16 streaming warps
 
-// Shared memory: [cap x es] columns | ent[2][cap] | xold[2][cap] | u[n4] |
-// dold[n4] | dnext[n4] | wred[kUrRows x n4]
+// Shared memory: [cap x es] columns | ent[2][cap] | xold[2][cap] | keep[cap] |
+// u[n4] | dold[n4] | dnext[n4] | wred[kUrRows x n4]
 __host__ __device__ inline size_t ur_fixed_bytes(int n) {
   const int n4 = ur_n4(n);
   return size_t(n4) * 4 * 3 + size_t(kUrRows) * n4 * 4;
 }
 
 int update_res_capacity(int n) {
-  const size_t per = size_t(ur_es(n)) * 4 + 16;
+  const size_t per = size_t(ur_es(n)) * 4 + 20;
   const size_t fixed = ur_fixed_bytes(n);
   if (fixed + per * 16 > kUrSmemMax) return 0;
   // a multiple of 4 keeps u, dold, dnext and wred (read as float4) 16-byte aligned
   return int((kUrSmemMax - fixed) / per) & ~3;
 }
 
-size_t update_res_smem_bytes(int n, int cap) { return size_t(cap) * (size_t(ur_es(n)) * 4 + 16) + ur_fixed_bytes(n); }
+size_t update_res_smem_bytes(int n, int cap) { return size_t(cap) * (size_t(ur_es(n)) * 4 + 20) + ur_fixed_bytes(n); }
 
 // Bounded spin of thread 0 until *ctr >= target.  False on timeout or when an
 // error is already flagged.
@@ -81,20 +81,23 @@ KSVD_DEV bool ur_wait_count(const unsigned* ctr, unsigned target, GridBarrier* f
   return true;
 }
 
-__host__ __device__ inline int ur_active(int c, int G) {
-  const int a = (c + kUrTargetSlice - 1) / kUrTargetSlice;
+__host__ __device__ inline int ur_active(int c, int G, int target) {
+  const int a = (c + target - 1) / target;
   return a < G ? a : G;
 }
 
 // residual_kernel: R = Y - X D, one warp per patch.  The patch's atoms and
 // coefficients sit in lanes 0..L-1 and are broadcast by shuffles; each lane
 // forms 16-byte pieces of the row with the support atoms' loads in flight
-// together (same FMA order as r = y - sum_s x_s d_s, s ascending).
+// together (same FMA order as r = y - sum_s x_s d_s, s ascending).  last[p]
+// (optional) receives the highest atom of the patch's support (-1 if none):
+// the sweep visits atoms in ascending order, so no atom after that one reads
+// the patch's residual row again in the sweep.
 __global__ void __launch_bounds__(256) residual_kernel(const float* __restrict__ Y, int64_t N, int n,
                                                        const float* __restrict__ D, int K, int L,
                                                        const int32_t* __restrict__ idx,
                                                        const float* __restrict__ coef, float* __restrict__ R,
-                                                       int vec4) {
+                                                       int* __restrict__ last, int vec4) {
   const int lane = threadIdx.x & 31;
   const int64_t warps = int64_t(gridDim.x) * (blockDim.x >> 5);
   for (int64_t p = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); p < N; p += warps) {
@@ -104,6 +107,12 @@ __global__ void __launch_bounds__(256) residual_kernel(const float* __restrict__
       a = __ldg(idx + p * L + lane);
       x = __ldg(coef + p * L + lane);
       if (a < 0 || a >= K || x == 0.0f) a = -1;
+    }
+    if (last) {
+      int top = a;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) top = max(top, __shfl_xor_sync(0xffffffffu, top, o));
+      if (lane == 0) last[p] = top;
     }
     if (vec4) {
       const int F = n >> 2;
@@ -163,7 +172,8 @@ template <int NW>
 __global__ void __launch_bounds__(kUrThreads, 1)
     update_res_kernel(float* R, int n, float* D, int K, int L, float* coef, const int* __restrict__ atom_ptr,
                       const int* __restrict__ entries, int q1_cap, int cap, float* gw, unsigned* sync,
-                      GridBarrier* flags, DevStats* stats, int timers) {
+                      GridBarrier* flags, DevStats* stats, int timers, const int* __restrict__ last,
+                      int slice_target) {
   extern __shared__ __align__(16) unsigned char ursm[];
   const int n4 = ur_n4(n), es = ur_es(n);
   const int F = n4 / 4, es4 = es / 4;  // float4 per row of u / w, per resident column
@@ -171,7 +181,8 @@ __global__ void __launch_bounds__(kUrThreads, 1)
   const float4* Es4 = reinterpret_cast<const float4*>(ursm);
   int* ent_b = reinterpret_cast<int*>(ursm + size_t(cap) * es * 4);  // [2][cap]
   float* xold_b = reinterpret_cast<float*>(ent_b + 2 * cap);           // [2][cap]
-  float* u = xold_b + 2 * cap;
+  int* keep = reinterpret_cast<int*>(xold_b + 2 * cap);  // residual row stored back (per resident column)
+  float* u = reinterpret_cast<float*>(keep + cap);
   float* dold = u + n4;
   float* dnext = dold + n4;
   float* wred = dnext + n4;  // [kUrRows][n4]
@@ -223,7 +234,7 @@ __global__ void __launch_bounds__(kUrThreads, 1)
   auto slice_of = [&](int a, int& beg, int& c, int& active, int& sb, int& se) {
     beg = atom_ptr[a];
     c = atom_ptr[a + 1] - beg;
-    active = ur_active(c, G);
+    active = ur_active(c, G, slice_target);
     sb = int(int64_t(c) * b / active);
     se = int(int64_t(c) * (b + 1) / active);
   };
@@ -583,6 +594,7 @@ __global__ void __launch_bounds__(kUrThreads, 1)
       const float x = (q < mc) ? dot_u(q) : 0.0f;
       v_s[q] = x;
       __stcg(coef + ent_s[q], x);
+      keep[q] = (last == nullptr || __ldg(last + ent_s[q] / L) != j) ? 1 : 0;
     }
     if (m > cap) {  // streamed columns: a warp per two columns
       float ur[NW];
@@ -609,18 +621,22 @@ __global__ void __launch_bounds__(kUrThreads, 1)
         if (q >= mc) x0 = 0.0f;
         if (q + kUrWarps >= mc) x1 = 0.0f;
         float* ra = R + int64_t(ea / L) * n;
+        if (last == nullptr || __ldg(last + ea / L) != j) {
 #pragma unroll
-        for (int k = 0; k < NW; ++k) {
-          const int i = lane + 32 * k;
-          if (i < n) __stcg(ra + i, fmaf(-x0, ur[k], e0[k]));
+          for (int k = 0; k < NW; ++k) {
+            const int i = lane + 32 * k;
+            if (i < n) __stcg(ra + i, fmaf(-x0, ur[k], e0[k]));
+          }
         }
         if (lane == 0) __stcg(coef + ea, x0);
         if (eb >= 0) {
           float* rb = R + int64_t(eb / L) * n;
+          if (last == nullptr || __ldg(last + eb / L) != j) {
 #pragma unroll
-          for (int k = 0; k < NW; ++k) {
-            const int i = lane + 32 * k;
-            if (i < n) __stcg(rb + i, fmaf(-x1, ur[k], e1[k]));
+            for (int k = 0; k < NW; ++k) {
+              const int i = lane + 32 * k;
+              if (i < n) __stcg(rb + i, fmaf(-x1, ur[k], e1[k]));
+            }
           }
           if (lane == 0) __stcg(coef + eb, x1);
         }
@@ -630,6 +646,7 @@ __global__ void __launch_bounds__(kUrThreads, 1)
     if (tma) {  // rows of 16-byte aligned float4
       for (int t = tid; t < mres * F; t += kUrThreads) {
         const int q = t / F, f = t - q * F;
+        if (!keep[q]) continue;
         const float x = v_s[q];
         const float4 e = Es4[size_t(q) * es4 + f], w = u4[f];
         float4 r;
@@ -642,7 +659,7 @@ __global__ void __launch_bounds__(kUrThreads, 1)
     } else {
       for (int t = tid; t < mres * n; t += kUrThreads) {
         const int q = t / n, i = t - q * n;
-        __stcg(R + int64_t(ent_s[q] / L) * n + i, fmaf(-v_s[q], u[i], Es[size_t(q) * es + i]));
+        if (keep[q]) __stcg(R + int64_t(ent_s[q] / L) * n + i, fmaf(-v_s[q], u[i], Es[size_t(q) * es + i]));
       }
     }
     fence_proxy_async_smem();  // generic accesses of Es before the next bulk copies into it
@@ -704,21 +721,23 @@ int update_res_grid_size(int n, int num_sms) {
 size_t update_res_partial_floats(int n, int grid) { return size_t(2) * grid * ur_n4(n); }
 
 cudaError_t launch_residual(const float* Y, int64_t N, int n, const float* D, int K, int L, const int32_t* idx,
-                            const float* coef, float* R, int num_sms, cudaStream_t s) {
+                            const float* coef, float* R, int* last, int num_sms, cudaStream_t s) {
   const int64_t want = (N + 7) / 8;
   const int blocks = int(want < int64_t(num_sms) * 16 ? want : int64_t(num_sms) * 16);
   const int vec4 = ((n & 3) == 0 && (reinterpret_cast<uintptr_t>(Y) & 15) == 0 &&
                     (reinterpret_cast<uintptr_t>(D) & 15) == 0 && (reinterpret_cast<uintptr_t>(R) & 15) == 0)
                        ? 1
                        : 0;
-  residual_kernel<<<blocks > 0 ? blocks : 1, 256, 0, s>>>(Y, N, n, D, K, L, idx, coef, R, vec4);
+  residual_kernel<<<blocks > 0 ? blocks : 1, 256, 0, s>>>(Y, N, n, D, K, L, idx, coef, R, last, vec4);
   return cudaGetLastError();
 }
 
 cudaError_t launch_update_res(float* R, int n, float* D, int K, int L, float* coef, const int* atom_ptr,
                               const int* entries, int q1_cap, float* gw, unsigned* sync, GridBarrier* flags,
-                              DevStats* stats, int timers, int grid, cudaStream_t s) {
+                              DevStats* stats, int timers, const int* last, int slice_target, int grid,
+                              cudaStream_t s) {
   void* fn = pick_update_res(n);
+  if (slice_target < 1) slice_target = kUrDefaultSlice;
   const int cap = update_res_capacity(n);
   if (!fn || cap < 16 || grid < 1) return cudaErrorInvalidValue;
   const size_t smem = update_res_smem_bytes(n, cap);
@@ -727,9 +746,10 @@ cudaError_t launch_update_res(float* R, int n, float* D, int K, int L, float* co
   e = cudaMemsetAsync(sync, 0, size_t(2) * K * sizeof(unsigned), s);
   if (e != cudaSuccess) return e;
   int capv = cap;
-  void* args[] = {(void*)&R,       (void*)&n,       (void*)&D,      (void*)&K,    (void*)&L,
-                  (void*)&coef,    (void*)&atom_ptr, (void*)&entries, (void*)&q1_cap, (void*)&capv,
-                  (void*)&gw,      (void*)&sync,    (void*)&flags,  (void*)&stats,   (void*)&timers};
+  void* args[] = {(void*)&R,     (void*)&n,        (void*)&D,       (void*)&K,      (void*)&L,
+                  (void*)&coef,  (void*)&atom_ptr, (void*)&entries, (void*)&q1_cap, (void*)&capv,
+                  (void*)&gw,    (void*)&sync,     (void*)&flags,   (void*)&stats,  (void*)&timers,
+                  (void*)&last,  (void*)&slice_target};
   return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kUrThreads), args, smem, s);
 }
 

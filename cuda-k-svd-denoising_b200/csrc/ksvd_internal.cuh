@@ -1,6 +1,7 @@
 // Internal declarations shared by the CUDA translation units of ksvd_sm100.
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <map>
@@ -107,13 +108,77 @@ cudaError_t launch_accumulate_phases(const DevStats* src, DevStats* dst, cudaStr
 bool update_res_supported(int n);
 int update_res_grid_size(int n, int num_sms);
 size_t update_res_partial_floats(int n, int grid);
+// last (optional, N ints): the highest atom of each patch's support, -1 if none.
 cudaError_t launch_residual(const float* Y, int64_t N, int n, const float* D, int K, int L, const int32_t* idx,
-                            const float* coef, float* R, int num_sms, cudaStream_t s);
+                            const float* coef, float* R, int* last, int num_sms, cudaStream_t s);
 // sync: 2K unsigned words (zeroed by the launch); gw: update_res_partial_floats.
 // stats receives the counters always, the phase times when timers != 0.
+// last (optional): from launch_residual; a residual row is not stored back by
+// the patch's last atom.  slice_target: entries per CTA before another CTA
+// joins an atom (<= 0: the default, 64).
 cudaError_t launch_update_res(float* R, int n, float* D, int K, int L, float* coef, const int* atom_ptr,
                               const int* entries, int q1_cap, float* gw, unsigned* sync, GridBarrier* flags,
-                              DevStats* stats, int timers, int grid, cudaStream_t s);
+                              DevStats* stats, int timers, const int* last, int slice_target, int grid,
+                              cudaStream_t s);
+
+// ---------------------------------------------------------------------------
+// Learned support proposal (kernels_mlp.cu, kernels_omp_restricted.cu).
+// ---------------------------------------------------------------------------
+enum GemmEpi : int {
+  kEpiF32 = 0,       // C -> c_f32
+  kEpiBiasF32 = 1,   // C + bias -> c_f32
+  kEpiBiasGelu = 2,  // z = C + bias -> c_f32 (optional), GELU(z) -> c_bf16
+  kEpiGeluBack = 3,  // C * GELU'(aux) -> c_bf16
+  kEpiTopK = 4,      // C + bias: the ktop largest of the first n_valid columns -> topk
+};
+constexpr int kMaxTopK = 16;
+
+// C[M x N] = A[M x K] . B[N x K]^T, BF16 operands, FP32 accumulation.  With a
+// K-contiguous operand element (r, k) is at P[r * ld + k], otherwise at
+// P[k * ld + r].  N and K multiples of 16; N <= 256 or a multiple of 256.
+struct GemmArgs {
+  const __nv_bfloat16* A;
+  long long lda;
+  const __nv_bfloat16* B;
+  long long ldb;
+  int M, N, K;
+  const float* bias;
+  float* c_f32;
+  long long ldc_f32;
+  __nv_bfloat16* c_bf16;
+  long long ldc_bf16;
+  const float* aux;
+  long long ld_aux;
+  int32_t* topk;
+  int ktop, n_valid;
+  GridBarrier* flags;
+};
+bool gemm_shape_ok(const GemmArgs& g, bool a_kcontig, bool b_kcontig);
+cudaError_t launch_gemm(const GemmArgs& g, bool a_kcontig, bool b_kcontig, int epi, cudaStream_t s);
+cudaError_t launch_mlp_input(const float* Y, int64_t B, int n, int np16, const int64_t* rows, int64_t mod,
+                             __nv_bfloat16* X, cudaStream_t s);
+cudaError_t launch_mlp_bce(const float* Z, int64_t B, int K, int K16, const int32_t* sup, int L, const int64_t* rows,
+                           __nv_bfloat16* dZ, double* loss_sum, cudaStream_t s);
+cudaError_t launch_mlp_colsum(const __nv_bfloat16* G, int64_t B, int C, int ld, float* out, cudaStream_t s);
+cudaError_t launch_mlp_adam(float* w, const float* grad, float* m1, float* m2, int64_t count, float lr, int step,
+                            cudaStream_t s);
+cudaError_t launch_mlp_to_bf16(const float* w, int rows, int cols, int rows_pad, int ld, __nv_bfloat16* out,
+                               cudaStream_t s);
+cudaError_t launch_mlp_unpad(const float* src, int rows, int cols, int ld, float* dst, cudaStream_t s);
+
+// OMP restricted to C candidate atoms per patch (exact FP64 correlations of
+// the candidates); patches whose residual norm ends above sqrt(thr2) are
+// appended to fb_list (fb_count counts them).
+cudaError_t launch_omp_restricted(const float* patches, int64_t N, int n, const float* dict, const double* gram,
+                                  int K, int L, const int32_t* cand, int C, double thr2, int32_t* idx, float* coef,
+                                  int64_t* fb_list, unsigned long long* fb_count, int num_sms, cudaStream_t s);
+bool omp_restricted_supported(int n, int L, int C);
+// Gather rows list[0..count) of src (row width w floats) into dst; scatter the
+// codes of the gathered rows back into the N x L idx / coef.
+cudaError_t launch_gather_rows(const float* src, int w, const int64_t* list, int64_t count, float* dst,
+                               cudaStream_t s);
+cudaError_t launch_scatter_codes(const int32_t* sidx, const float* scoef, int L, const int64_t* list, int64_t count,
+                                 int32_t* idx, float* coef, cudaStream_t s);
 
 // Image rebuild.
 cudaError_t launch_col2im(const float* noisy, const PatchGeom& g, const float* dict, int K, int L,
@@ -154,6 +219,19 @@ struct ksvd_ctx {
   std::map<std::string, Family> families;
   std::vector<cudaEvent_t> event_pool;
   int64_t launch_count = 0;
+  int upd_slice = 0;  // entries per CTA of the update sweep (0: the kernel's default; ksvd_autotune)
+
+  // Learned support proposal (proposal.cu): shapes, state and the noise
+  // variance behind the fallback threshold; its device buffers are named
+  // workspace buffers ("prop_*").
+  struct Proposal {
+    bool ready = false;  // weights present (initialised, set or trained)
+    int n = 0, n16 = 0, K = 0, K16 = 0, H = 0;
+    int64_t nparams = 0;
+    int64_t steps = 0;    // Adam steps taken
+    double sigma2 = 0.0;  // noise variance (<= 0: not set)
+    int64_t last_fallbacks = 0, total_fallbacks = 0, last_patches = 0;
+  } prop;
 
   ksvd::GridBarrier* d_flags = nullptr;  // error flag word + barrier
   ksvd::DevStats* d_stats = nullptr;      // per-call counters

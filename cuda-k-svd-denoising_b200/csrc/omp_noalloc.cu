@@ -20,9 +20,14 @@
 //     to start at zero, but two calls whose work overlaps on the GPU (for
 //     example on two streams) overwrite each other's Gram and give wrong
 //     codes: serialise them;
+//   * the OMP kernel is the one ksvd_omp's FP32 form would run: the
+//     dictionary resident in shared memory when it fits, else streamed through
+//     it (so every patch size that ksvd_omp accepts works up to 512 atoms);
 //   * the first call on each device looks up the array's device address
 //     (cudaGetSymbolAddress, with that device current) and caches it; make
-//     that first call before starting any stream capture.
+//     that first call before starting any stream capture.  The cached address
+//     belongs to the device's primary context: after cudaDeviceReset() it is
+//     stale and this entry point must not be called again in that process.
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -76,7 +81,8 @@ extern "C" ksvd_status ksvd_omp_noalloc(const ksvd_params* p, const float* d_pat
   const int n = int(n64), K = p->atoms, L = p->omp_iter;
   if (K < 1 || L < 1 || L > 32) return KSVD_ERR_INVALID;
   if (K > kNoAllocMaxAtoms) return KSVD_ERR_TOO_LARGE;
-  if (!ksvd::omp_fp32_supported(n, K, L)) return KSVD_ERR_INVALID;
+  const bool resident = ksvd::omp_fp32_supported(n, K, L);
+  if (!resident && !ksvd::omp_stream_supported(n, K, L)) return KSVD_ERR_INVALID;
   int device = 0;
   if (cudaGetDevice(&device) != cudaSuccess) {
     cudaGetLastError();
@@ -91,9 +97,13 @@ extern "C" ksvd_status ksvd_omp_noalloc(const ksvd_params* p, const float* d_pat
     return KSVD_ERR_CUDA;
   }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (ksvd::launch_gram_f64(d_dict, K, n, gram, s) != cudaSuccess ||
-      ksvd::launch_omp_fp32(d_patches, num_patches, n, d_dict, gram, K, L, d_idx, d_coef, num_sms, nullptr, s) !=
-          cudaSuccess) {
+  cudaError_t e = ksvd::launch_gram_f64(d_dict, K, n, gram, s);
+  if (e == cudaSuccess)
+    e = resident ? ksvd::launch_omp_fp32(d_patches, num_patches, n, d_dict, gram, K, L, d_idx, d_coef, num_sms,
+                                         nullptr, s)
+                 : ksvd::launch_omp_stream(d_patches, num_patches, n, d_dict, gram, K, L, d_idx, d_coef, num_sms,
+                                           nullptr, s);
+  if (e != cudaSuccess) {
     cudaGetLastError();
     return KSVD_ERR_CUDA;
   }

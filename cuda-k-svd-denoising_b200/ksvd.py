@@ -24,7 +24,9 @@ OK, ERR_LOAD, ERR_DENOISE, ERR_SAVE = 0, -1, -2, -3
 ERR_INVALID, ERR_CUDA, ERR_NO_MEMORY, ERR_TIMEOUT, ERR_NUMERIC, ERR_NO_DEVICE = -10, -11, -12, -13, -14, -15
 ERR_TOO_LARGE = -16
 # ksvd_precision
-PREC_FP32, PREC_BF16_RESCORE, PREC_FP16_RESCORE = 0, 1, 2
+PREC_FP32, PREC_BF16_RESCORE, PREC_FP16_RESCORE, PREC_BF16_LEARNED = 0, 1, 2, 3
+# learned proposal
+PROPOSAL_HIDDEN, PROPOSAL_CANDIDATES, PROPOSAL_FALLBACK = 512, 16, 1.15
 # compat flags
 COMPAT_INT_NORM, COMPAT_Q1_CAP = 0x1, 0x2
 COMPAT_REFERENCE = COMPAT_INT_NORM | COMPAT_Q1_CAP
@@ -68,6 +70,34 @@ class KsvdStats(ctypes.Structure):
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class ProposalStats(ctypes.Structure):
+    _fields_ = [
+        ("pairs", ctypes.c_int64),
+        ("steps", ctypes.c_int64),
+        ("first_loss", ctypes.c_double),
+        ("final_loss", ctypes.c_double),
+        ("collect_ms", ctypes.c_double),
+        ("train_ms", ctypes.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class TuneResult(ctypes.Structure):
+    _fields_ = [
+        ("update_slice", ctypes.c_int),
+        ("candidates", ctypes.c_int),
+        ("slice", ctypes.c_int * 8),
+        ("update_ms", ctypes.c_double * 8),
+    ]
+
+    def as_dict(self) -> dict:
+        k = self.candidates
+        return {"update_slice": self.update_slice,
+                "update_ms_by_slice": {int(self.slice[i]): float(self.update_ms[i]) for i in range(k)}}
 
 
 class KsvdError(RuntimeError):
@@ -154,6 +184,34 @@ def lib():
         L.ksvd_run_batch.restype = _int
         L.ksvd_omp_noalloc.argtypes = [P, _vp, _i64, _vp, _vp, _vp, _vp]
         L.ksvd_omp_noalloc.restype = _int
+        _u64 = ctypes.c_uint64
+        PS = ctypes.POINTER(ProposalStats)
+        L.ksvd_proposal_num_params.argtypes = [P]
+        L.ksvd_proposal_num_params.restype = _i64
+        L.ksvd_proposal_init.argtypes = [_vp, _u64]
+        L.ksvd_proposal_init.restype = _int
+        L.ksvd_proposal_set_params.argtypes = [_vp, _vp, _i64]
+        L.ksvd_proposal_set_params.restype = _int
+        L.ksvd_proposal_get_params.argtypes = [_vp, _vp, _i64]
+        L.ksvd_proposal_get_params.restype = _int
+        L.ksvd_proposal_loss_grad.argtypes = [_vp, _vp, _i64, _vp, ctypes.POINTER(ctypes.c_double), _vp]
+        L.ksvd_proposal_loss_grad.restype = _int
+        L.ksvd_proposal_train.argtypes = [_vp, _vp, _i64, _vp, _int, _int, _int, ctypes.c_float, _u64, PS]
+        L.ksvd_proposal_train.restype = _int
+        L.ksvd_proposal_fit.argtypes = [_vp, _vp, _i64, _vp, _int, _int, _u64, PS]
+        L.ksvd_proposal_fit.restype = _int
+        L.ksvd_proposal_candidates.argtypes = [_vp, _vp, _i64, _vp]
+        L.ksvd_proposal_candidates.restype = _int
+        L.ksvd_omp_restricted.argtypes = [_vp, _vp, _i64, _vp, _vp, _int, _vp, _vp, ctypes.POINTER(_i64)]
+        L.ksvd_omp_restricted.restype = _int
+        L.ksvd_set_noise_variance.argtypes = [_vp, ctypes.c_float]
+        L.ksvd_set_noise_variance.restype = _int
+        L.ksvd_proposal_fallbacks.argtypes = [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i64)]
+        L.ksvd_proposal_fallbacks.restype = _int
+        L.ksvd_autotune.argtypes = [_vp, _vp, _i64, _vp, ctypes.POINTER(TuneResult)]
+        L.ksvd_autotune.restype = _int
+        L.ksvd_set_update_slice.argtypes = [_vp, _int]
+        L.ksvd_set_update_slice.restype = _int
         _lib = L
     return _lib
 
@@ -315,6 +373,68 @@ class Context:
 
     def launch_count(self) -> int:
         return int(lib().ksvd_launch_count(self.h))
+
+    # -- autotuning --------------------------------------------------------
+    def autotune(self, patches, dictionary) -> dict:
+        r = TuneResult()
+        self._check(lib().ksvd_autotune(self.h, _ptr(patches), patches.shape[0], _ptr(dictionary),
+                                        ctypes.byref(r)))
+        return r.as_dict()
+
+    def set_update_slice(self, slice_: int):
+        self._check(lib().ksvd_set_update_slice(self.h, int(slice_)))
+
+    # -- learned support proposal -----------------------------------------
+    def proposal_num_params(self) -> int:
+        return int(lib().ksvd_proposal_num_params(ctypes.byref(self.params)))
+
+    def proposal_init(self, seed: int = 0):
+        self._check(lib().ksvd_proposal_init(self.h, int(seed)))
+
+    def proposal_set_params(self, params: np.ndarray):
+        params = np.ascontiguousarray(params, dtype=np.float32)
+        self._check(lib().ksvd_proposal_set_params(self.h, params.ctypes.data, params.size))
+
+    def proposal_get_params(self) -> np.ndarray:
+        out = np.empty(self.proposal_num_params(), np.float32)
+        self._check(lib().ksvd_proposal_get_params(self.h, out.ctypes.data, out.size))
+        return out
+
+    def proposal_loss_grad(self, patches, supports, grad) -> float:
+        loss = ctypes.c_double(0.0)
+        self._check(lib().ksvd_proposal_loss_grad(self.h, _ptr(patches), patches.shape[0], _ptr(supports),
+                                                  ctypes.byref(loss), _ptr(grad)))
+        return loss.value
+
+    def proposal_train(self, patches, supports, T: int, epochs: int, batch: int = 4096, lr: float = 1e-3,
+                       seed: int = 0) -> dict:
+        st = ProposalStats()
+        self._check(lib().ksvd_proposal_train(self.h, _ptr(patches), patches.shape[0], _ptr(supports), int(T),
+                                              int(epochs), int(batch), float(lr), int(seed), ctypes.byref(st)))
+        return st.as_dict()
+
+    def proposal_fit(self, patches, dictionary, iters: int, epochs: int = 2, seed: int = 0) -> dict:
+        st = ProposalStats()
+        self._check(lib().ksvd_proposal_fit(self.h, _ptr(patches), patches.shape[0], _ptr(dictionary), int(iters),
+                                            int(epochs), int(seed), ctypes.byref(st)))
+        return st.as_dict()
+
+    def proposal_candidates(self, patches, cand):
+        self._check(lib().ksvd_proposal_candidates(self.h, _ptr(patches), patches.shape[0], _ptr(cand)))
+
+    def omp_restricted(self, patches, dictionary, cand, idx, coef) -> int:
+        above = _i64(0)
+        self._check(lib().ksvd_omp_restricted(self.h, _ptr(patches), patches.shape[0], _ptr(dictionary), _ptr(cand),
+                                              cand.shape[1], _ptr(idx), _ptr(coef), ctypes.byref(above)))
+        return above.value
+
+    def set_noise_variance(self, sigma2: float):
+        self._check(lib().ksvd_set_noise_variance(self.h, float(sigma2)))
+
+    def proposal_fallbacks(self) -> dict:
+        a, b, c = _i64(0), _i64(0), _i64(0)
+        self._check(lib().ksvd_proposal_fallbacks(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return {"last": a.value, "total": b.value, "patches": c.value}
 
 
 def omp_noalloc(params: KsvdParams, patches, dictionary, idx, coef, stream_handle: int | None = None) -> int:

@@ -78,7 +78,12 @@ typedef enum ksvd_status {
 typedef enum ksvd_precision {
   KSVD_PREC_FP32 = 0,         /* plain FP32 FMA                              */
   KSVD_PREC_BF16_RESCORE = 1, /* BF16 tensor cores + exact re-score         */
-  KSVD_PREC_FP16_RESCORE = 2  /* FP16 tensor cores + exact re-score         */
+  KSVD_PREC_FP16_RESCORE = 2, /* FP16 tensor cores + exact re-score         */
+  KSVD_PREC_BF16_LEARNED = 3  /* learned top-16 proposal (BF16 MLP on the
+                                 tensor cores) + OMP restricted to it, exact
+                                 FP64 scores; patches whose residual stays
+                                 above the threshold are re-coded by the
+                                 BF16 + re-score OMP (see ksvd_proposal_*)  */
 } ksvd_precision;
 
 /* Reference behaviours reproduced on request (bit flags for ksvd_params.compat). */
@@ -138,7 +143,7 @@ int ksvd_type_from_string(const char* name, int* known);
 const char* ksvd_type_name(int type);
 
 /* Replaces Denoiser::factory (denoiser.cpp:108-127) + the parameter copy of
- * BatchDenoiser::factory (batch_denoiser.cpp:385-399).  Validates p, selects
+ * BatchDenoiser::factory (batch_denoiser.cpp:36-118).  Validates p, selects
  * the device and creates the context's stream.  Device memory is allocated
  * on first use and kept for the life of the context. */
 ksvd_status ksvd_create(const ksvd_params* p, ksvd_ctx** out);
@@ -238,14 +243,104 @@ ksvd_status ksvd_profile_counters(ksvd_ctx* ctx, int64_t* out, int count);
  * n) and the outputs idx / coef (num_patches x omp_iter), all on the current
  * device, and the stream (NULL = legacy default stream).  The dictionary Gram
  * lives in a 2 MiB array compiled into the library, so atoms is limited to
- * 512 (KSVD_ERR_TOO_LARGE beyond).  Every call on a device shares that array:
- * calls whose work overlaps on the GPU (e.g. on two streams) race; serialise
- * them.  The first call on each device looks the array's address up and
- * caches it; make it before starting any stream capture.
+ * 512 (KSVD_ERR_TOO_LARGE beyond) for every patch size that ksvd_omp accepts
+ * (the dictionary is streamed through shared memory when it does not fit
+ * there).  Every call on a device shares that array: calls whose work
+ * overlaps on the GPU (e.g. on two streams) race; serialise them.  The first
+ * call on each device looks the array's address up and caches it; make it
+ * before starting any stream capture.  The cached address belongs to the
+ * device's primary context: do not call this again after cudaDeviceReset().
  * It has no counterpart in the reference (whose OMP allocates on every call,
  * cublas_matrix_omp.cu:79,125-165,254-255). */
 ksvd_status ksvd_omp_noalloc(const ksvd_params* p, const float* d_patches, int64_t num_patches,
                              const float* d_dict, int32_t* d_idx, float* d_coef, void* stream);
+
+/* ---- autotuning -------------------------------------------------------------
+ * The update sweep splits each atom's patches over CTAs of about `slice`
+ * entries each; the best slice depends on the workload (patch size, support
+ * sizes).  ksvd_autotune times one sweep with each candidate slice on the
+ * caller's patches and dictionary (codes from one OMP call of the context's
+ * form), keeps the fastest in the context and reports them all.  Results
+ * differ between slices only in the summation order of the partial sums. */
+#define KSVD_TUNE_MAX 8
+typedef struct ksvd_tune_result {
+  int update_slice;                /* the slice chosen */
+  int candidates;                  /* number of slices timed */
+  int slice[KSVD_TUNE_MAX];        /* the slices */
+  double update_ms[KSVD_TUNE_MAX]; /* device time of one sweep with each */
+} ksvd_tune_result;
+ksvd_status ksvd_autotune(ksvd_ctx* ctx, const float* d_patches, int64_t num_patches, const float* d_dict,
+                          ksvd_tune_result* out);
+/* Sets the slice directly (0 = the default, 64). */
+ksvd_status ksvd_set_update_slice(ksvd_ctx* ctx, int slice);
+
+/* ---- learned support proposal --------------------------------------------
+ * A small network proposes, for each patch, the KSVD_PROPOSAL_CANDIDATES atoms
+ * most likely to be in its OMP support; the OMP of precision
+ * KSVD_PREC_BF16_LEARNED then picks its atoms among those candidates only
+ * (argmax over the candidates of the exact correlations, the reference's
+ * least squares and stopping rule), and every patch whose final residual
+ * norm exceeds KSVD_PROPOSAL_FALLBACK * sqrt(sigma2 * n) is re-coded by the
+ * full OMP.  The reference has no counterpart: its OMP scores every atom
+ * (cublas_matrix_omp.cu:193-233).
+ *
+ * Network: x = y sqrt(n) / |y|  ->  512 (GELU)  ->  512 (GELU)  ->  atoms
+ * (sigmoid scores); BF16 weights and activations, FP32 accumulation, FP32
+ * master weights trained with Adam on the binary cross-entropy between the
+ * scores and the support mask.  Parameters, in this order, row-major:
+ * W1 [512 x n], b1 [512], W2 [512 x 512], b2 [512], W3 [atoms x 512],
+ * b3 [atoms].  The atoms' identities are those of the dictionary the
+ * supports came from: a proposal is trained for one image's dictionary
+ * trajectory (ksvd_proposal_fit) and used on that image. */
+#define KSVD_PROPOSAL_HIDDEN 512
+#define KSVD_PROPOSAL_CANDIDATES 16
+#define KSVD_PROPOSAL_FALLBACK 1.15
+
+typedef struct ksvd_proposal_stats {
+  int64_t pairs;     /* (patch, support) pairs trained on per epoch */
+  int64_t steps;     /* optimiser steps taken */
+  double first_loss; /* mean loss of the first 1% of the steps */
+  double final_loss; /* mean loss of the last 1% of the steps */
+  double collect_ms; /* device time generating the pairs (fit only) */
+  double train_ms;   /* device time of the training steps */
+} ksvd_proposal_stats;
+
+/* Number of network parameters for these patch and dictionary sizes. */
+int64_t ksvd_proposal_num_params(const ksvd_params* p);
+/* Random initial weights (uniform +-1/sqrt(fan_in), zero biases) from seed. */
+ksvd_status ksvd_proposal_init(ksvd_ctx* ctx, uint64_t seed);
+/* Host FP32 parameter vector in / out (count = ksvd_proposal_num_params). */
+ksvd_status ksvd_proposal_set_params(ksvd_ctx* ctx, const float* params, int64_t count);
+ksvd_status ksvd_proposal_get_params(ksvd_ctx* ctx, float* params, int64_t count);
+/* Mean loss and its gradient (FP32, parameter order above, device buffer
+ * d_grad of num_params floats) for the batch d_patches [B x n] with supports
+ * d_supports [B x omp_iter] (-1 = unused slot); B a multiple of 16. */
+ksvd_status ksvd_proposal_loss_grad(ksvd_ctx* ctx, const float* d_patches, int64_t B, const int32_t* d_supports,
+                                    double* loss, float* d_grad);
+/* Trains on the T x N pairs (patch p, supports row t * N + p of d_supports
+ * [T x N x omp_iter]) for `epochs` passes in seeded random order, minibatches
+ * of `batch` pairs (a multiple of 16), Adam with learning rate lr. */
+ksvd_status ksvd_proposal_train(ksvd_ctx* ctx, const float* d_patches, int64_t N, const int32_t* d_supports, int T,
+                                int epochs, int batch, float lr, uint64_t seed, ksvd_proposal_stats* stats);
+/* Generates the pairs with the plain FP32 method, collect_iters K-SVD
+ * iterations from d_dict (left unchanged), the supports of each iteration's
+ * OMP, and trains on them (fresh weights from seed, epochs passes). */
+ksvd_status ksvd_proposal_fit(ksvd_ctx* ctx, const float* d_patches, int64_t N, const float* d_dict,
+                              int collect_iters, int epochs, uint64_t seed, ksvd_proposal_stats* stats);
+/* The network's top KSVD_PROPOSAL_CANDIDATES atoms per patch, best first
+ * (d_cand: N x KSVD_PROPOSAL_CANDIDATES). */
+ksvd_status ksvd_proposal_candidates(ksvd_ctx* ctx, const float* d_patches, int64_t N, int32_t* d_cand);
+/* OMP restricted to C candidates per patch (d_cand: N x C, C <= 16), no
+ * fallback; *above (may be NULL) receives the number of patches whose
+ * residual norm ends above the fallback threshold (needs the noise variance). */
+ksvd_status ksvd_omp_restricted(ksvd_ctx* ctx, const float* d_patches, int64_t N, const float* d_dict,
+                                const int32_t* d_cand, int C, int32_t* d_idx, float* d_coef, int64_t* above);
+/* Noise variance behind the fallback threshold of the learned OMP
+ * (ksvd_denoise sets it from its sigma2 argument). */
+ksvd_status ksvd_set_noise_variance(ksvd_ctx* ctx, float sigma2);
+/* Patches re-coded by the full OMP: in the last learned OMP call, and in all
+ * calls since the context was created; *patches: patches of the last call. */
+ksvd_status ksvd_proposal_fallbacks(const ksvd_ctx* ctx, int64_t* last, int64_t* total, int64_t* patches);
 
 /* ---- config.json (batch_denoiser.cpp:36-118) ------------------------------
  * The reference's keys: inputFolder, outputFolder, files[] {name, ref, and

@@ -327,3 +327,39 @@ def test_subimage_errors(torch_cuda, ksvd, synth):
         with pytest.raises(ksvd.KsvdError) as e:
             c.denoise(img, 100.0)
         assert e.value.status == ksvd.ERR_INVALID
+
+
+@pytest.mark.parametrize("precision", [0, 2])
+def test_denoise_rectangular_vs_fp64_oracle(torch_cuda, ksvd, oracle, synth, precision):
+    """Rectangular patches on a non-square image: 5 (along y) x 7 (along x)
+    patches at steps 3 (y) and 2 (x) on a 128 (x) x 100 (y) image, 48 atoms,
+    L = 4, 3 iterations; PSNR within 0.05 dB of the FP64 oracle with the same
+    (consistent) geometry."""
+    clean = synth.clean_image(128, 61)[:100, :]
+    noisy = synth.add_gaussian(clean, 20.0, 61)
+    kw = dict(patch_width_dim=5, patch_height_dim=7, sliding_width=3, sliding_height=2, atoms=48, omp_iter=4,
+              ksvd_iter=3, compat=1, precision=precision)
+    with mkctx(ksvd, **kw) as c:
+        out, st = c.denoise(noisy, 400.0)
+    ref, info = oracle.ksvd_denoise(noisy, 400.0, pw=5, ph=7, sw=3, sh=2, atoms=48, ksvd_iter=3, omp_iter=4,
+                                    q1_cap=False, int_norm=True)
+    pg, pr = synth.psnr(clean, out), synth.psnr(clean, ref)
+    assert abs(pg - pr) <= 0.05, (pg, pr)
+    assert pg > synth.psnr(clean, noisy) + 1.0
+    assert st["num_patches"] == oracle.num_patches(128, 100, 5, 7, 3, 2)
+
+
+def test_build_image_rectangular_vs_oracle(torch_cuda, ksvd, oracle, synth):
+    """createImage with 5 x 7 patches (steps 3 x 2) on a 128 x 100 image: the
+    rebuilt pixels within 1e-5 relative of the oracle, lambda within 1e-5."""
+    img = synth.add_gaussian(synth.clean_image(128, 62)[:100, :], 20.0, 62)
+    Y = oracle.extract_patches(img, 5, 7, 3, 2)
+    D = oracle.init_dictionary(Y, 24, dtype=np.float32)
+    idx, coef = oracle.omp(Y, D, 3, dtype=np.float32)
+    c = mkctx(ksvd, patch_width_dim=5, patch_height_dim=7, sliding_width=3, sliding_height=2, atoms=24, omp_iter=3)
+    out = torch_cuda.empty(img.shape, dtype=torch_cuda.float32, device="cuda")
+    lam = c.build_image(dev(torch_cuda, img), 400.0, dev(torch_cuda, D), dev(torch_cuda, idx), dev(torch_cuda, coef),
+                        out)
+    ref, rlam = oracle.build_image(img, 5, 7, 3, 2, D, idx, coef, 400.0, dtype=np.float32)
+    assert lam == pytest.approx(rlam, rel=1e-5)
+    np.testing.assert_allclose(out.cpu().numpy(), ref, rtol=1e-5, atol=1e-3)

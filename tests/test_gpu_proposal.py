@@ -1,0 +1,179 @@
+"""The learned support proposal on the GPU against its CPU oracle
+(oracle/mlp_oracle.py, itself pinned by finite differences):
+
+* loss and every gradient block of the tensor-core forward/backward pass
+  (BF16 operands, FP32 accumulation) against the float64 oracle with the
+  same BF16 rounding points: loss within 1e-4 relative, each block within
+  2e-2 relative (Frobenius);
+* the network's top-16 candidates against the oracle's scores;
+* the restricted OMP against the oracle's restricted pursuit, and against
+  the full FP64 OMP when the true support is among the candidates;
+* what training buys: on the 512^2 workload a proposal fitted on the plain
+  method's supports agrees with the full FP64 OMP far more often, and falls
+  back far less, than the same network untrained."""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def mlp():
+    from ksvd_loader import load_oracle
+    load_oracle()
+    import mlp_oracle
+    return mlp_oracle
+
+
+def dev(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def _ctx(ksvd, K=256, patch=12, step=3, L=5, precision=3):
+    return ksvd.Context(ksvd.make_params(patch_width_dim=patch, patch_height_dim=patch, sliding_width=step,
+                                         sliding_height=step, atoms=K, omp_iter=L, precision=precision))
+
+
+@pytest.fixture(scope="module")
+def batch(synth, oracle):
+    img = synth.add_gaussian(synth.clean_image(96, 41), 20.0, 41)
+    Y = oracle.extract_patches(img, 12, 12, 3, 3)[:512]  # 512 patches of 144 values
+    D = oracle.init_dictionary(oracle.extract_patches(img, 12, 12, 3, 3), 256, int_norm=True, dtype=np.float32)
+    sup, _ = oracle.omp(Y.astype(np.float64), D.astype(np.float64), 5)
+    return Y, D, sup
+
+
+def _params(mlp, n, K, seed, scale=None):
+    rng = np.random.default_rng(seed)
+    P = mlp.num_params(n, K)
+    p = np.zeros(P, np.float32)
+    o = 0
+    for rows, fan in ((512, n), (512, None), (512, 512), (512, None), (K, 512), (K, None)):
+        size = rows * (fan or 1)
+        lim = (1.0 / np.sqrt(fan)) if fan else 0.05
+        p[o:o + size] = rng.uniform(-lim, lim, size)
+        o += size
+    return p
+
+
+def test_proposal_loss_grad_vs_oracle(torch_cuda, ksvd, mlp, batch):
+    torch = torch_cuda
+    Y, D, sup = batch
+    c = _ctx(ksvd)
+    P = c.proposal_num_params()
+    params = _params(mlp, 144, 256, 7)
+    assert P == params.size
+    c.proposal_set_params(params)
+    np.testing.assert_array_equal(c.proposal_get_params(), params)
+    grad = torch.zeros(P, dtype=torch.float32, device="cuda")
+    loss = c.proposal_loss_grad(dev(torch, Y), dev(torch, sup), grad)
+    rl, rg = mlp.loss_grad(params.astype(np.float64), Y, sup, 256, emulate=True)
+    assert abs(loss - rl) <= 1e-4 * abs(rl), (loss, rl)
+    g = grad.cpu().numpy().astype(np.float64)
+    o = np.cumsum([0, 512 * 144, 512, 512 * 512, 512, 256 * 512, 256])
+    for name, a, b in zip(("W1", "b1", "W2", "b2", "W3", "b3"), o[:-1], o[1:]):
+        err = np.linalg.norm(g[a:b] - rg[a:b]) / (np.linalg.norm(rg[a:b]) + 1e-30)
+        assert err <= 2e-2, (name, err)
+    c.close()
+
+
+def test_proposal_candidates_vs_oracle(torch_cuda, ksvd, mlp, batch):
+    torch = torch_cuda
+    Y, _, _ = batch
+    c = _ctx(ksvd)
+    params = _params(mlp, 144, 256, 11)
+    c.proposal_set_params(params)
+    cand = torch.empty((Y.shape[0], 16), dtype=torch.int32, device="cuda")
+    c.proposal_candidates(dev(torch, Y), cand)
+    torch.cuda.synchronize()
+    got = cand.cpu().numpy()
+    Z = mlp.forward(params.astype(np.float64), Y, 256, emulate=True)["Z3"]
+    ref = mlp.top_candidates(Z, 16)
+    same = np.mean([set(a) == set(b) for a, b in zip(got, ref)])
+    assert same >= 0.95, same
+    # every candidate scores within a hair of the oracle's 16th best
+    kth = np.sort(Z, axis=1)[:, -16]
+    sc = np.take_along_axis(Z, got.astype(np.int64), axis=1)
+    assert np.all(sc >= kth[:, None] - 1e-3 * (1.0 + np.abs(kth[:, None])))
+    assert np.all((got >= 0) & (got < 256))
+    assert all(len(set(r)) == 16 for r in got)
+    c.close()
+
+
+def test_omp_restricted_vs_oracle(torch_cuda, ksvd, mlp, oracle, synth):
+    torch = torch_cuda
+    img = synth.add_gaussian(synth.clean_image(96, 43), 20.0, 43)
+    Y = oracle.extract_patches(img, 12, 12, 3, 3)
+    D = oracle.init_dictionary(Y, 256, int_norm=True, dtype=np.float32)
+    N = Y.shape[0]
+    rng = np.random.default_rng(5)
+    full_i, full_c = oracle.omp(Y.astype(np.float64), D.astype(np.float64), 5)
+    # candidates: the full pursuit's support plus random other atoms, shuffled
+    cand = np.empty((N, 16), np.int32)
+    for p in range(N):
+        s = [a for a in full_i[p] if a >= 0]
+        rest = rng.permutation(np.setdiff1d(np.arange(256), s))[:16 - len(s)]
+        cand[p] = rng.permutation(np.concatenate([s, rest]))
+    c = _ctx(ksvd)
+    c.set_noise_variance(400.0)
+    idx = torch.empty((N, 5), dtype=torch.int32, device="cuda")
+    coef = torch.empty((N, 5), dtype=torch.float32, device="cuda")
+    above = c.omp_restricted(dev(torch, Y), dev(torch, D), dev(torch, cand), idx, coef)
+    gi, gc = idx.cpu().numpy(), coef.cpu().numpy()
+    agree = np.mean(np.all(gi == full_i, axis=1))
+    assert agree >= 0.999, agree
+    m = np.all(gi == full_i, axis=1)
+    rel = np.abs(gc[m] - full_c[m]) / (np.abs(full_c[m]).max(axis=1, keepdims=True) + 1e-30)
+    assert rel.max() < 1e-4
+    # against the oracle's restricted pursuit with random candidates
+    cand2 = np.stack([rng.permutation(256)[:16] for _ in range(N)]).astype(np.int32)
+    c.omp_restricted(dev(torch, Y), dev(torch, D), dev(torch, cand2), idx, coef)
+    ri, rc, rn = mlp.omp_restricted(Y, D.astype(np.float64), cand2, 5)
+    gi2, gc2 = idx.cpu().numpy(), coef.cpu().numpy()
+    assert np.mean(np.all(gi2 == ri, axis=1)) >= 0.999
+    m = np.all(gi2 == ri, axis=1)
+    rel = np.abs(gc2[m] - rc[m]) / (np.abs(rc[m]).max(axis=1, keepdims=True) + 1e-30)
+    assert rel.max() < 1e-4
+    thr = 1.15 * np.sqrt(400.0 * 144)
+    above2 = c.omp_restricted(dev(torch, Y), dev(torch, D), dev(torch, cand2), idx, coef)
+    assert abs(above2 - int(np.sum(rn > thr))) <= max(2, int(0.002 * N))
+    assert above <= above2
+    c.close()
+
+
+def test_learned_fit_gain(torch_cuda, ksvd, oracle, synth):
+    """The 512^2 workload (27,889 patches of 144, 256 atoms, L = 5): fit the
+    proposal on 4 plain iterations' supports (2 epochs), then compare the
+    learned OMP from the initial dictionary with the full FP64 OMP, beside
+    the same network untrained."""
+    torch = torch_cuda
+    w = synth.WORKLOADS["img512_p12s3_k256"]
+    clean, noisy = w.images()
+    Y = oracle.extract_patches(noisy, 12, 12, 3, 3)
+    D = oracle.init_dictionary(Y, 256, int_norm=True, dtype=np.float32)
+    N = Y.shape[0]
+    full_i, _ = oracle.omp(Y.astype(np.float64), D.astype(np.float64), 5)
+    Yd, Dd = dev(torch, Y), dev(torch, D)
+
+    def learned(c):
+        c.set_noise_variance(w.sigma ** 2)
+        idx = torch.empty((N, 5), dtype=torch.int32, device="cuda")
+        coef = torch.empty((N, 5), dtype=torch.float32, device="cuda")
+        c.omp(Yd, Dd, idx, coef)
+        torch.cuda.synchronize()
+        fb = c.proposal_fallbacks()
+        return float(np.mean(np.all(idx.cpu().numpy() == full_i, axis=1))), fb["last"] / N
+
+    c = _ctx(ksvd)
+    st = c.proposal_fit(Yd, Dd, iters=4, epochs=2, seed=1)
+    assert st["final_loss"] < 0.7 * st["first_loss"], st
+    a_t, f_t = learned(c)
+    u = _ctx(ksvd)
+    u.proposal_init(1)
+    a_u, f_u = learned(u)
+    assert a_t >= 0.9, (a_t, f_t, a_u, f_u)
+    assert a_t >= a_u + 0.3, (a_t, a_u)
+    assert f_t <= f_u, (f_t, f_u)
+    c.close()
+    u.close()
