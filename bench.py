@@ -232,6 +232,45 @@ def quality_vs_fp64(pkg, oracle, wl, clean, noisy, D0, patches, make_ctx, forms)
     return res
 
 
+def batch_workload(pkg, ksvd, count=64, tune=True):
+    """The uneven batch (64 seeded images, sides 256..2048, patches 8/12/22
+    at stride 3, 16 speckle): ksvd_denoise_many end to end (host images in
+    and out), beside the same images denoised one by one with ksvd_denoise in
+    the same run.  Rate = patches x iterations / device time of the batch's
+    iterations."""
+    import torch
+    jobs = pkg.synth.many_workload(count=count)
+    specs = []
+    for j in jobs:
+        prm = ksvd.make_params(patch_width_dim=j["patch"], patch_height_dim=j["patch"], sliding_width=j["stride"],
+                               sliding_height=j["stride"], atoms=j["atoms"], omp_iter=j["omp_iter"],
+                               ksvd_iter=j["ksvd_iter"], speckle=int(j["speckle"]), compat=1,
+                               precision=ksvd.PREC_FP16_RESCORE)
+        specs.append((prm, j["noisy"], j["sigma2"]))
+    ksvd.denoise_many(specs[:2], tune=False)  # warm-up (module load, first allocations)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    outs, st = ksvd.denoise_many(specs, tune=tune)
+    wall_batch = time.perf_counter() - t
+    t = time.perf_counter()
+    for prm, img, s2 in specs:
+        with ksvd.Context(prm) as c:
+            c.denoise(img, s2)
+    wall_seq = time.perf_counter() - t
+    T = jobs[0]["ksvd_iter"]
+    psnr_gain = [pkg.synth.psnr(j["clean"], o) - pkg.synth.psnr(j["clean"], j["noisy"]) for j, o in zip(jobs, outs)]
+    return {"images": count, "patches": st["num_patches"], "ksvd_iter": T,
+            "sides": sorted({j["side"] for j in jobs}), "patch_sides": sorted({j["patch"] for j in jobs}),
+            "speckle_images": sum(j["speckle"] for j in jobs),
+            "iter_patches_per_s": st["num_patches"] * T / (st["iter_ms"] / 1000.0),
+            "iter_ms": st["iter_ms"], "call_device_ms": st["total_ms"], "call_wall_s": wall_batch,
+            "sequential_wall_s": wall_seq, "speedup_vs_one_by_one": wall_seq / wall_batch,
+            "graph": st["graph"], "streams": st["streams"], "split_alpha": st["split_alpha"],
+            "update_ctas_min_max": [min(st["update_ctas"]), max(st["update_ctas"])],
+            "psnr_gain_db_min_median": [float(np.min(psnr_gain)), float(np.median(psnr_gain))],
+            "form": "fp16 (22x22 patches: FP32 streamed OMP)"}
+
+
 def run_reference(args, wl):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -288,6 +327,7 @@ def main():
     ap.add_argument("--e2e-calls", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=40.0)
+    ap.add_argument("--no-batch", action="store_true", help="skip the 64-image uneven batch workload")
     ap.add_argument("--no-quality", action="store_true",
                     help="skip the accuracy report against the FP64 oracle (about a minute of CPU)")
     args = ap.parse_args()
@@ -508,6 +548,9 @@ def main():
         if not args.no_cpu_baseline:
             oracle = load_oracle()
             cpu, _ = cpu_baseline(pkg, oracle, wl, budget_s=args.cpu_budget)
+        batch = None
+        if not args.no_batch and world == 1:
+            batch = batch_workload(pkg, ksvd)
         acc = None
         if not args.no_quality and world == 1:
             acc = quality_vs_fp64(pkg, load_oracle(), wl, clean, noisy, D0.cpu().numpy(), patches, make_ctx,
@@ -561,6 +604,7 @@ def main():
                         "vs_fp64_oracle": acc},
             "forms_patches_per_s": forms,
             "metric_by_form": by_form,
+            "extra_workloads": {"batch64_uneven": batch},
             "clocks": clk_summary,
         }
         if cpu:

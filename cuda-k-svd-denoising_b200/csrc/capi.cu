@@ -308,6 +308,13 @@ ksvd_status omp_form(ksvd_ctx* c, const float* d_patches, int64_t N, const float
             ksvd::launch_omp_tc(d_patches, N, n, d_dict, gram, K, L, d_idx, d_coef, c->num_sms,
                                 precision == KSVD_PREC_FP16_RESCORE ? 1 : 0, c->d_flags, ph, c->stream),
             "omp (tensor cores)");
+  } else if (precision != KSVD_PREC_FP32 && ksvd::omp_tcb_supported(n, K, L)) {
+    void* scratch = nullptr;
+    KSVD_TRY(ws(c, "tcb_scratch", ksvd::omp_tcb_scratch_bytes(n, K), &scratch));
+    KSVD_CU(c,
+            ksvd::launch_omp_tcb(d_patches, N, n, d_dict, gram, K, L, d_idx, d_coef, c->num_sms,
+                                 precision == KSVD_PREC_FP16_RESCORE ? 1 : 0, scratch, c->d_flags, ph, c->stream),
+            "omp (tensor cores, streamed dictionary)");
   } else if (ksvd::omp_fp32_supported(n, K, L)) {
     KSVD_CU(c, ksvd::launch_omp_fp32(d_patches, N, n, d_dict, gram, K, L, d_idx, d_coef, c->num_sms, ph, c->stream),
             "omp");
@@ -343,8 +350,8 @@ ksvd_status ksvd_omp(ksvd_ctx* c, const float* d_patches, int64_t N, const float
 namespace ksvd {
 namespace api {
 
-ksvd_status update_form(ksvd_ctx* c, const float* d_patches, int64_t N, float* d_dict, const int32_t* d_idx,
-                        float* d_coef) {
+ksvd_status update_prepare(ksvd_ctx* c, const float* d_patches, int64_t N, float* d_dict, const int32_t* d_idx,
+                           float* d_coef, int ctas, ksvd::UpdGroup* g) {
   const int n = c->p.patch_width_dim * c->p.patch_height_dim, K = c->p.atoms, L = c->p.omp_iter;
   ksvd::CsrWork w;
   w.nchunks = ksvd::csr_num_chunks(N);
@@ -352,12 +359,10 @@ ksvd_status update_form(ksvd_ctx* c, const float* d_patches, int64_t N, float* d
   KSVD_TRY(wsT(c, "csr_atom_ptr", size_t(2) * K + 1, &w.atom_ptr));
   KSVD_TRY(wsT(c, "csr_entries", size_t(N) * L, &w.entries));
   w.records = nullptr;  // the residual-based sweep needs only the entries
-  const int grid = ksvd::update_res_grid_size(n, c->num_sms);
-  if (grid < 1) return fail(c, KSVD_ERR_CUDA, "update kernel cannot be made co-resident");
   float *resid = nullptr, *gw = nullptr;
   unsigned* sync = nullptr;
   KSVD_TRY(wsT(c, "upd_resid", size_t(N) * n, &resid));
-  KSVD_TRY(wsT(c, "upd_partials", ksvd::update_res_partial_floats(n, grid), &gw));
+  KSVD_TRY(wsT(c, "upd_partials", ksvd::update_res_partial_floats(n, ctas), &gw));
   KSVD_TRY(wsT(c, "upd_sync", size_t(2) * K, &sync));
   int* last = nullptr;
   KSVD_TRY(wsT(c, "upd_last", size_t(N), &last));
@@ -371,12 +376,37 @@ ksvd_status update_form(ksvd_ctx* c, const float* d_patches, int64_t N, float* d
             ksvd::launch_residual(d_patches, N, n, d_dict, K, L, d_idx, d_coef, resid, last, c->num_sms, c->stream),
             "residual");
   }
+  std::memset(g, 0, sizeof(*g));
+  g->R = resid;
+  g->D = d_dict;
+  g->coef = d_coef;
+  g->atom_ptr = w.atom_ptr;
+  g->entries = w.entries;
+  g->last = last;
+  g->gw = gw;
+  g->sync = sync;
+  g->n = n;
+  g->K = K;
+  g->L = L;
+  g->q1_cap = (c->p.compat & KSVD_COMPAT_Q1_CAP) ? 1 : 0;
+  g->cap = ksvd::update_res_capacity(n);
+  g->ctas = ctas;
+  g->slice_target = c->upd_slice;
+  return KSVD_OK;
+}
+
+ksvd_status update_form(ksvd_ctx* c, const float* d_patches, int64_t N, float* d_dict, const int32_t* d_idx,
+                        float* d_coef) {
+  const int n = c->p.patch_width_dim * c->p.patch_height_dim;
+  const int grid = ksvd::update_res_grid_size(n, c->num_sms);
+  if (grid < 1) return fail(c, KSVD_ERR_CUDA, "update kernel cannot be made co-resident");
+  ksvd::UpdBatch b;
+  std::memset(&b, 0, sizeof(b));
+  b.ngroups = 1;
+  KSVD_TRY(update_prepare(c, d_patches, N, d_dict, d_idx, d_coef, grid, &b.g[0]));
   KSVD_CU(c, cudaMemsetAsync(c->d_stats, 0, sizeof(ksvd::DevStats), c->stream), "stats reset");
   Prof pr(c, "update", 1);
-  KSVD_CU(c,
-          ksvd::launch_update_res(resid, n, d_dict, K, L, d_coef, w.atom_ptr, w.entries,
-                                  (c->p.compat & KSVD_COMPAT_Q1_CAP) ? 1 : 0, gw, sync, c->d_flags, c->d_stats,
-                                  c->profiling >= 2 ? 1 : 0, last, c->upd_slice, grid, c->stream),
+  KSVD_CU(c, ksvd::launch_update_batch(b, c->d_flags, c->d_stats, c->profiling >= 2 ? 1 : 0, grid, c->stream),
           "update");
   if (c->profiling) {
     // fold this sweep's phase timers into the profiling accumulator

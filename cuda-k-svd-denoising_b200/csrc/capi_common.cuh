@@ -130,6 +130,10 @@ ksvd_status omp_form(ksvd_ctx* c, const float* d_patches, int64_t N, const float
                      float* d_coef, int precision);
 ksvd_status update_form(ksvd_ctx* c, const float* d_patches, int64_t N, float* d_dict, const int32_t* d_idx,
                         float* d_coef);
+// The CSR and residual of one sweep (on the context's stream) and its group
+// descriptor for launch_update_batch with `ctas` CTAs (cta_begin left 0).
+ksvd_status update_prepare(ksvd_ctx* c, const float* d_patches, int64_t N, float* d_dict, const int32_t* d_idx,
+                           float* d_coef, int ctas, ksvd::UpdGroup* g);
 ksvd_status proposal_candidates_impl(ksvd_ctx* c, const float* d_patches, int64_t N, int32_t* d_cand);
 ksvd_status omp_learned_impl(ksvd_ctx* c, const float* d_patches, int64_t N, const float* d_dict, const double* gram,
                              int32_t* d_idx, float* d_coef);

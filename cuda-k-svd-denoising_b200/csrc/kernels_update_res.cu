@@ -28,6 +28,8 @@
 // waits are bounded.
 #include <cuda_runtime.h>
 
+#include <cstring>
+
 #include "device_util.cuh"
 #include "ksvd_internal.cuh"
 
@@ -168,13 +170,26 @@ KSVD_DEV void red_release_add(unsigned* p, unsigned v) {
   asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+// One launch sweeps one or several problems (images): group g owns the CTAs
+// [cta_begin, cta_begin + ctas) and walks its own atoms with its own buffers,
+// counters and partials; groups never wait on one another.
 template <int NW>
 __global__ void __launch_bounds__(kUrThreads, 1)
-    update_res_kernel(float* R, int n, float* D, int K, int L, float* coef, const int* __restrict__ atom_ptr,
-                      const int* __restrict__ entries, int q1_cap, int cap, float* gw, unsigned* sync,
-                      GridBarrier* flags, DevStats* stats, int timers, const int* __restrict__ last,
-                      int slice_target) {
+    update_res_kernel(const UpdBatch batch, GridBarrier* flags, DevStats* stats, int timers) {
   extern __shared__ __align__(16) unsigned char ursm[];
+  int gi = 0;
+  while (gi + 1 < batch.ngroups && int(blockIdx.x) >= batch.g[gi + 1].cta_begin) ++gi;
+  const UpdGroup& grp = batch.g[gi];
+  float* const R = grp.R;
+  float* const D = grp.D;
+  float* const coef = grp.coef;
+  const int* __restrict__ const atom_ptr = grp.atom_ptr;
+  const int* __restrict__ const entries = grp.entries;
+  const int* __restrict__ const last = grp.last;
+  float* const gw = grp.gw;
+  unsigned* const sync = grp.sync;
+  const int n = grp.n, K = grp.K, L = grp.L, q1_cap = grp.q1_cap, cap = grp.cap;
+  const int slice_target = grp.slice_target > 0 ? grp.slice_target : kUrDefaultSlice;
   const int n4 = ur_n4(n), es = ur_es(n);
   const int F = n4 / 4, es4 = es / 4;  // float4 per row of u / w, per resident column
   float* Es = reinterpret_cast<float*>(ursm);
@@ -194,7 +209,7 @@ __global__ void __launch_bounds__(kUrThreads, 1)
   __shared__ __align__(8) unsigned long long s_mbar;  // completion of the residual-row bulk copies
   __shared__ unsigned long long s_ph[8];  // phase times of this CTA (slots 0..7)
 
-  const int G = int(gridDim.x), b = int(blockIdx.x);
+  const int G = grp.ctas, b = int(blockIdx.x) - grp.cta_begin;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   unsigned* iter_cnt = sync;
   unsigned* done_cnt = sync + K;
@@ -211,7 +226,7 @@ __global__ void __launch_bounds__(kUrThreads, 1)
   __syncthreads();
 
   // phase times gather in shared memory and are flushed once at the end
-  const bool timer = (timers != 0 && b == 0 && tid == 0);
+  const bool timer = (timers != 0 && blockIdx.x == 0 && tid == 0);
   if (timer)
     for (int k = 0; k < 8; ++k) s_ph[k] = 0ull;
   unsigned long long tmark = timer ? globaltimer_ns() : 0ull;
@@ -732,25 +747,64 @@ cudaError_t launch_residual(const float* Y, int64_t N, int n, const float* D, in
   return cudaGetLastError();
 }
 
+cudaError_t launch_update_batch(const UpdBatch& batch, GridBarrier* flags, DevStats* stats, int timers, int grid,
+                                cudaStream_t s) {
+  if (batch.ngroups < 1 || batch.ngroups > kUpdMaxGroups || grid < 1) return cudaErrorInvalidValue;
+  int nmax = 0;
+  for (int i = 0; i < batch.ngroups; ++i) {
+    const UpdGroup& g = batch.g[i];
+    if (g.ctas < 1 || g.cta_begin < 0 || g.cta_begin + g.ctas > grid) return cudaErrorInvalidValue;
+    if (i > 0 && g.cta_begin != batch.g[i - 1].cta_begin + batch.g[i - 1].ctas) return cudaErrorInvalidValue;
+    if (g.cap < 16 || g.cap > update_res_capacity(g.n)) return cudaErrorInvalidValue;
+    nmax = g.n > nmax ? g.n : nmax;
+  }
+  if (batch.g[0].cta_begin != 0 || batch.g[batch.ngroups - 1].cta_begin + batch.g[batch.ngroups - 1].ctas != grid)
+    return cudaErrorInvalidValue;
+  void* fn = pick_update_res(nmax);
+  if (!fn) return cudaErrorInvalidValue;
+  size_t smem = 0;
+  for (int i = 0; i < batch.ngroups; ++i) {
+    const size_t b = update_res_smem_bytes(batch.g[i].n, batch.g[i].cap);
+    smem = b > smem ? b : smem;
+  }
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  for (int i = 0; i < batch.ngroups; ++i) {
+    e = cudaMemsetAsync(batch.g[i].sync, 0, size_t(2) * batch.g[i].K * sizeof(unsigned), s);
+    if (e != cudaSuccess) return e;
+  }
+  UpdBatch b = batch;
+  void* args[] = {(void*)&b, (void*)&flags, (void*)&stats, (void*)&timers};
+  return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kUrThreads), args, smem, s);
+}
+
 cudaError_t launch_update_res(float* R, int n, float* D, int K, int L, float* coef, const int* atom_ptr,
                               const int* entries, int q1_cap, float* gw, unsigned* sync, GridBarrier* flags,
                               DevStats* stats, int timers, const int* last, int slice_target, int grid,
                               cudaStream_t s) {
-  void* fn = pick_update_res(n);
-  if (slice_target < 1) slice_target = kUrDefaultSlice;
   const int cap = update_res_capacity(n);
-  if (!fn || cap < 16 || grid < 1) return cudaErrorInvalidValue;
-  const size_t smem = update_res_smem_bytes(n, cap);
-  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-  if (e != cudaSuccess) return e;
-  e = cudaMemsetAsync(sync, 0, size_t(2) * K * sizeof(unsigned), s);
-  if (e != cudaSuccess) return e;
-  int capv = cap;
-  void* args[] = {(void*)&R,     (void*)&n,        (void*)&D,       (void*)&K,      (void*)&L,
-                  (void*)&coef,  (void*)&atom_ptr, (void*)&entries, (void*)&q1_cap, (void*)&capv,
-                  (void*)&gw,    (void*)&sync,     (void*)&flags,   (void*)&stats,  (void*)&timers,
-                  (void*)&last,  (void*)&slice_target};
-  return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kUrThreads), args, smem, s);
+  if (cap < 16 || grid < 1) return cudaErrorInvalidValue;
+  UpdBatch b;
+  std::memset(&b, 0, sizeof(b));
+  b.ngroups = 1;
+  UpdGroup& g = b.g[0];
+  g.R = R;
+  g.D = D;
+  g.coef = coef;
+  g.atom_ptr = atom_ptr;
+  g.entries = entries;
+  g.last = last;
+  g.gw = gw;
+  g.sync = sync;
+  g.n = n;
+  g.K = K;
+  g.L = L;
+  g.q1_cap = q1_cap;
+  g.cap = cap;
+  g.cta_begin = 0;
+  g.ctas = grid;
+  g.slice_target = slice_target;
+  return launch_update_batch(b, flags, stats, timers, grid, s);
 }
 
 }  // namespace ksvd

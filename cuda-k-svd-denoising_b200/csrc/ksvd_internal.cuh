@@ -88,6 +88,15 @@ cudaError_t launch_omp_tc(const float* patches, int64_t N, int n, const float* d
                           int L, int32_t* idx, float* coef, int num_sms, int fp16, GridBarrier* flags,
                           DevStats* stats, cudaStream_t s);
 
+// OMP with the 16-bit tensor-core correlation for dictionaries beyond the
+// resident kernel (atoms <= 512, n <= 256): the 16-bit dictionary streams
+// from `scratch` (omp_tcb_scratch_bytes, written by the launch).
+bool omp_tcb_supported(int n, int K, int L);
+size_t omp_tcb_scratch_bytes(int n, int K);
+cudaError_t launch_omp_tcb(const float* patches, int64_t N, int n, const float* dict, const double* gram, int K,
+                           int L, int32_t* idx, float* coef, int num_sms, int fp16, void* scratch,
+                           GridBarrier* flags, DevStats* stats, cudaStream_t s);
+
 // Dictionary update.
 struct CsrWork {
   int* chunk_counts;   // nchunks x K
@@ -113,6 +122,31 @@ cudaError_t launch_residual(const float* Y, int64_t N, int n, const float* D, in
                             const float* coef, float* R, int* last, int num_sms, cudaStream_t s);
 // sync: 2K unsigned words (zeroed by the launch); gw: update_res_partial_floats.
 // stats receives the counters always, the phase times when timers != 0.
+// One problem of a (multi-problem) update sweep: its buffers (as for
+// launch_update_res; gw: 2 x ctas x round4(n) floats, sync: 2K words, zeroed
+// by the launch), sizes, the resident-column capacity (update_res_capacity(n)
+// or less) and its CTAs [cta_begin, cta_begin + ctas) of the launch.
+struct UpdGroup {
+  float* R;
+  float* D;
+  float* coef;
+  const int* atom_ptr;
+  const int* entries;
+  const int* last;
+  float* gw;
+  unsigned* sync;
+  int n, K, L, q1_cap, cap, cta_begin, ctas, slice_target;
+};
+constexpr int kUpdMaxGroups = 64;
+struct UpdBatch {
+  int ngroups;
+  UpdGroup g[kUpdMaxGroups];
+};
+int update_res_capacity(int n);
+// One cooperative launch of `grid` CTAs (one per SM at most) over all groups;
+// the groups' CTA ranges must tile [0, grid) in order.
+cudaError_t launch_update_batch(const UpdBatch& batch, GridBarrier* flags, DevStats* stats, int timers, int grid,
+                                cudaStream_t s);
 // last (optional): from launch_residual; a residual row is not stored back by
 // the patch's last atom.  slice_target: entries per CTA before another CTA
 // joins an atom (<= 0: the default, 64).

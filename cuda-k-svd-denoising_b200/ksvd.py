@@ -100,6 +100,34 @@ class TuneResult(ctypes.Structure):
                 "update_ms_by_slice": {int(self.slice[i]): float(self.update_ms[i]) for i in range(k)}}
 
 
+class ImageJob(ctypes.Structure):
+    _fields_ = [
+        ("params", KsvdParams),
+        ("img", ctypes.c_void_p),
+        ("out", ctypes.c_void_p),
+        ("width", ctypes.c_int),
+        ("height", ctypes.c_int),
+        ("sigma2", ctypes.c_float),
+    ]
+
+
+class ManyStats(ctypes.Structure):
+    _fields_ = [
+        ("num_patches", ctypes.c_int64),
+        ("iter_ms", ctypes.c_double),
+        ("total_ms", ctypes.c_double),
+        ("graph", ctypes.c_int),
+        ("streams", ctypes.c_int),
+        ("split_alpha", ctypes.c_double),
+        ("update_ctas", ctypes.c_int * 64),
+    ]
+
+    def as_dict(self, count: int) -> dict:
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "update_ctas"}
+        d["update_ctas"] = [int(self.update_ctas[i]) for i in range(count)]
+        return d
+
+
 class KsvdError(RuntimeError):
     def __init__(self, status: int, message: str):
         super().__init__(f"ksvd status {status}: {message}")
@@ -212,6 +240,8 @@ def lib():
         L.ksvd_autotune.restype = _int
         L.ksvd_set_update_slice.argtypes = [_vp, _int]
         L.ksvd_set_update_slice.restype = _int
+        L.ksvd_denoise_many.argtypes = [ctypes.POINTER(ImageJob), _int, _int, _int, ctypes.POINTER(ManyStats)]
+        L.ksvd_denoise_many.restype = _int
         _lib = L
     return _lib
 
@@ -435,6 +465,29 @@ class Context:
         a, b, c = _i64(0), _i64(0), _i64(0)
         self._check(lib().ksvd_proposal_fallbacks(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
         return {"last": a.value, "total": b.value, "patches": c.value}
+
+
+def denoise_many(jobs, device: int = 0, tune: bool = True, outs=None):
+    """ksvd_denoise_many over [(params, image (H, W) float32, sigma2), ...].
+    Returns (list of denoised images, stats dict)."""
+    arr = (ImageJob * len(jobs))()
+    keep = []
+    out_list = []
+    for i, (params, img, sigma2) in enumerate(jobs):
+        img = np.ascontiguousarray(img, dtype=np.float32)
+        out = outs[i] if outs is not None else np.empty_like(img)
+        keep.append(img)
+        out_list.append(out)
+        arr[i].params = params
+        arr[i].img = img.ctypes.data
+        arr[i].out = out.ctypes.data
+        arr[i].height, arr[i].width = img.shape
+        arr[i].sigma2 = float(sigma2)
+    st = ManyStats()
+    rc = lib().ksvd_denoise_many(arr, len(jobs), int(device), int(bool(tune)), ctypes.byref(st))
+    if rc != OK:
+        raise KsvdError(rc, lib().ksvd_status_string(rc).decode())
+    return out_list, st.as_dict(len(jobs))
 
 
 def omp_noalloc(params: KsvdParams, patches, dictionary, idx, coef, stream_handle: int | None = None) -> int:

@@ -104,3 +104,36 @@ WORKLOADS = {
     # patch matrix: larger than L2, a few hundred MB on the device)
     "img1536_p12s3_k256": Workload("img1536_p12s3_k256", 1536, 25.0, 12, 3, 256, 5, 10),
 }
+
+
+def many_workload(count: int = 64, seed: int = 2024, sides=(256, 512, 1024, 1536, 2048), patches=(8, 12, 22),
+                  stride: int = 3, speckle_count: int = 16, atoms: int = 256, omp_iter: int = 5, ksvd_iter: int = 10):
+    """The uneven batch: `count` seeded images with sides drawn uniformly from
+    `sides`, patch sides from `patches` at `stride`; the first `speckle_count`
+    (in a seeded order) get multiplicative Gamma noise of shape 4 (denoised in
+    the log2 domain), the others Gaussian noise with sigma uniform in [10, 40].
+    Returns a list of dicts: clean, noisy, side, patch, speckle, sigma2 (the
+    noise variance handed to the denoiser; for speckle the variance of log2 of
+    Gamma(4, 1/4) noise)."""
+    rng = np.random.default_rng(seed)
+    speck = set(rng.permutation(count)[:speckle_count].tolist())
+    # variance of log2(g), g ~ Gamma(shape 4, mean 1): trigamma(4) / ln(2)^2
+    trigamma4 = np.pi ** 2 / 6.0 - (1.0 + 1.0 / 4.0 + 1.0 / 9.0)
+    var_log2 = trigamma4 / np.log(2.0) ** 2
+    out = []
+    for i in range(count):
+        side = int(rng.choice(sides))
+        patch = int(rng.choice(patches))
+        img_seed = int(rng.integers(0, 2 ** 31 - 1))
+        clean = clean_image(side, img_seed)
+        if i in speck:
+            clean = clean + 1.0  # strictly positive for the log domain
+            noisy = add_speckle(clean, 4.0, img_seed)
+            out.append(dict(clean=clean, noisy=noisy, side=side, patch=patch, stride=stride, speckle=True,
+                            sigma2=float(var_log2), atoms=atoms, omp_iter=omp_iter, ksvd_iter=ksvd_iter))
+        else:
+            sigma = float(rng.uniform(10.0, 40.0))
+            noisy = add_gaussian(clean, sigma, img_seed)
+            out.append(dict(clean=clean, noisy=noisy, side=side, patch=patch, stride=stride, speckle=False,
+                            sigma2=sigma * sigma, atoms=atoms, omp_iter=omp_iter, ksvd_iter=ksvd_iter))
+    return out

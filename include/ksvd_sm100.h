@@ -255,6 +255,38 @@ ksvd_status ksvd_profile_counters(ksvd_ctx* ctx, int64_t* out, int count);
 ksvd_status ksvd_omp_noalloc(const ksvd_params* p, const float* d_patches, int64_t num_patches,
                              const float* d_dict, int32_t* d_idx, float* d_coef, void* stream);
 
+/* ---- many images in one pipeline -------------------------------------------
+ * ksvd_denoise_many denoises up to 64 images of any size and patch shape
+ * (each with its own parameters, noise variance and dictionary) together: per
+ * K-SVD iteration the images' OMP, atom lists and residuals run concurrently
+ * on a pool of streams and one persistent launch sweeps the atoms of every
+ * image at once, the SMs split between the images by their sweep work.  The
+ * second and later iterations replay a CUDA graph of the whole batch
+ * iteration.  With tune != 0 the split is chosen by timing one sweep per
+ * candidate weighting on the first iteration's codes.  The per-image results
+ * equal ksvd_denoise's for the same parameters.  Every job must have the same
+ * ksvd_iter and device, no sub-images and not the learned form.  Replaces the
+ * reference's file-by-file loop (batch_denoiser.cpp:36-118, main.cpp:56-112). */
+typedef struct ksvd_image_job {
+  ksvd_params params; /* this image's parameters */
+  const float* img;   /* host, height x width (linear for speckle) */
+  float* out;         /* host, height x width */
+  int width, height;
+  float sigma2; /* noise variance */
+} ksvd_image_job;
+
+typedef struct ksvd_many_stats {
+  int64_t num_patches; /* all images */
+  double iter_ms;      /* device time of the K-SVD iterations of all images */
+  double total_ms;     /* device time of the whole call (uploads to downloads) */
+  int graph;           /* 1: iterations 2..T replayed from a CUDA graph */
+  int streams;         /* streams in the pool */
+  double split_alpha;  /* SMs split by (sweep bytes)^alpha */
+  int update_ctas[64]; /* CTAs of each image in the shared sweep */
+} ksvd_many_stats;
+
+ksvd_status ksvd_denoise_many(const ksvd_image_job* jobs, int count, int device, int tune, ksvd_many_stats* stats);
+
 /* ---- autotuning -------------------------------------------------------------
  * The update sweep splits each atom's patches over CTAs of about `slice`
  * entries each; the best slice depends on the workload (patch size, support

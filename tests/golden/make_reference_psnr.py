@@ -15,7 +15,9 @@ from pathlib import Path
 import numpy as np
 from PIL import Image
 
-REF = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference") / "test" / "images"
+if len(sys.argv) != 2:
+    sys.exit("usage: make_reference_psnr.py <path of the reference project>")
+REF = Path(sys.argv[1]) / "test" / "images"
 OUT = Path(__file__).resolve().parent / "reference_barbara_psnr.npz"
 
 

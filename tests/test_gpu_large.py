@@ -36,11 +36,12 @@ def check_omp(idx, coef, ri, rc):
     assert rel.max() < 1e-4, rel.max()
 
 
-@pytest.mark.parametrize("precision", [0, 2])
+@pytest.mark.parametrize("precision", [0, 1, 2])
 def test_omp_512_atoms_16x16(torch_cuda, ksvd, oracle, synth, precision):
     """n = 256, K = 512, L = 8 (the 4096^2 workload's dictionary shape): the
-    dictionary is streamed through shared memory; the tensor-core forms run
-    the FP32 kernel at this size."""
+    FP32 form streams the dictionary through shared memory; the 16-bit forms
+    stream 16-feature slices of the 16-bit dictionary through a ring of
+    shared-memory slots into 512 TMEM columns (kernels_omp_tcb.cu)."""
     noisy = synth.add_gaussian(synth.clean_image(128, 41), 15.0, 41)
     Y = oracle.extract_patches(noisy, 16, 16, 2, 2)
     D = oracle.init_dictionary(Y, 512, int_norm=True, dtype=np.float32)
@@ -150,3 +151,40 @@ def test_update_mixed_atom_sizes_deterministic(torch_cuda, ksvd, oracle, synth):
     err = np.abs(runs[0][0] - Dr).max()
     assert err < 1e-4, err
     assert np.abs(runs[0][1] - cr).max() < 1e-4 * np.abs(cr).max()
+
+
+@pytest.mark.parametrize("precision", [1, 2])
+def test_omp_tcb_shapes(torch_cuda, ksvd, oracle, synth, precision):
+    """The streamed tensor-core kernel at other shapes it serves: 300 atoms
+    of 12 x 12 patches (Kp = 304 columns, a partial last quarter), 400 atoms
+    of 10 x 10 patches (n not a multiple of 16), fewer patches than a tile."""
+    for side, patch, step, K, L, rows in ((96, 12, 3, 300, 5, None), (88, 10, 2, 400, 6, None),
+                                          (96, 12, 3, 300, 5, 77)):
+        noisy = synth.add_gaussian(synth.clean_image(side, 44 + K), 20.0, 44 + K)
+        Y = oracle.extract_patches(noisy, patch, patch, step, step)
+        D = oracle.init_dictionary(Y, K, int_norm=True, dtype=np.float32)
+        if rows:
+            Y = np.ascontiguousarray(Y[:rows])
+        idx, coef = run_omp(torch_cuda, ksvd, Y, D, patch_width_dim=patch, patch_height_dim=patch,
+                            sliding_width=step, sliding_height=step, atoms=K, omp_iter=L, precision=precision)
+        ri, rc = oracle.omp(Y.astype(np.float64), D.astype(np.float64), L)
+        check_omp(idx, coef, ri, rc)
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("precision", [0, 2])
+def test_denoise_img4096_shape_vs_fp64_oracle(torch_cuda, ksvd, oracle, synth, precision):
+    """The 4096^2 workload's settings (sigma 15, 16 x 16 patches at stride 2,
+    512 atoms, L = 8, 8 iterations) on a 256^2 image of the same generator
+    (14,641 patches): PSNR within 0.05 dB of the FP64 oracle."""
+    w = synth.WORKLOADS["img4096_p16s2_k512"]
+    clean = synth.clean_image(256, w.seed)
+    noisy = synth.add_gaussian(clean, w.sigma, w.seed)
+    kw = dict(patch_width_dim=16, patch_height_dim=16, sliding_width=2, sliding_height=2, atoms=512, omp_iter=8,
+              ksvd_iter=8, compat=1, precision=precision)
+    with mkctx(ksvd, **kw) as c:
+        out, _ = c.denoise(noisy, w.sigma ** 2)
+    ref, _ = oracle.ksvd_denoise(noisy, w.sigma ** 2, pw=16, ph=16, sw=2, sh=2, atoms=512, ksvd_iter=8, omp_iter=8,
+                                 q1_cap=False, int_norm=True)
+    pg, pr = synth.psnr(clean, out), synth.psnr(clean, ref)
+    assert abs(pg - pr) <= 0.05, (pg, pr)
