@@ -271,6 +271,53 @@ def batch_workload(pkg, ksvd, count=64, tune=True):
             "form": "fp16 (22x22 patches: FP32 streamed OMP)"}
 
 
+def workload_rates(pkg, ksvd, name, forms=("fp32", "fp16"), steps=3, warmup=1):
+    """Patches/s per K-SVD iteration of another workload (device-timed K
+    iterations from the initial dictionary after W warm-up ones), per form."""
+    import torch
+    wl = pkg.synth.WORKLOADS[name]
+    _, noisy = wl.images()
+    out = {"workload": name, "num_patches": wl.num_patches, "atoms": wl.atoms, "omp_iter": wl.omp_iter,
+           "patch": f"{wl.patch}x{wl.patch}", "stride": wl.stride, "steps": steps, "warmup": warmup}
+    precs = {"fp32": ksvd.PREC_FP32, "bf16": ksvd.PREC_BF16_RESCORE, "fp16": ksvd.PREC_FP16_RESCORE}
+    patches = D = D0 = idx = coef = None
+    for form in forms:
+        params = ksvd.make_params(patch_width_dim=wl.patch, patch_height_dim=wl.patch, sliding_width=wl.stride,
+                                  sliding_height=wl.stride, atoms=wl.atoms, omp_iter=wl.omp_iter, compat=1,
+                                  precision=precs[form])
+        with ksvd.Context(params) as c:
+            c.set_stream(torch.cuda.current_stream().cuda_stream)  # the events below are on this stream
+            if patches is None:
+                N = ksvd.num_patches(params, wl.size, wl.size)
+                patches = torch.empty((N, wl.n), dtype=torch.float32, device="cuda")
+                D = torch.empty((wl.atoms, wl.n), dtype=torch.float32, device="cuda")
+                idx = torch.empty((N, wl.omp_iter), dtype=torch.int32, device="cuda")
+                coef = torch.empty((N, wl.omp_iter), dtype=torch.float32, device="cuda")
+                c.extract_patches(torch.from_numpy(noisy).cuda(), patches)
+                c.init_dictionary(patches, D)
+                torch.cuda.synchronize()
+                D0 = D.clone()
+            D.copy_(D0)
+            torch.cuda.synchronize()
+            c.iterate(patches, D, idx, coef, warmup)
+            D.copy_(D0)
+            c.profile(1)
+            c.profile_reset()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            c.iterate(patches, D, idx, coef, steps)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / steps
+            fam = {f: c.profile_read(f)[0] / steps for f in ("gram", "omp", "csr", "residual", "update")}
+            out[form] = {"patches_per_s": wl.num_patches / (ms / 1000.0), "ms_per_step": ms,
+                         "kernel_ms_per_step": fam}
+    del patches, D, D0, idx, coef
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_reference(args, wl):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -548,9 +595,10 @@ def main():
         if not args.no_cpu_baseline:
             oracle = load_oracle()
             cpu, _ = cpu_baseline(pkg, oracle, wl, budget_s=args.cpu_budget)
-        batch = None
+        batch = big = None
         if not args.no_batch and world == 1:
             batch = batch_workload(pkg, ksvd)
+            big = workload_rates(pkg, ksvd, "img4096_p16s2_k512", forms=("fp32", "fp16", "bf16"))
         acc = None
         if not args.no_quality and world == 1:
             acc = quality_vs_fp64(pkg, load_oracle(), wl, clean, noisy, D0.cpu().numpy(), patches, make_ctx,
@@ -604,7 +652,7 @@ def main():
                         "vs_fp64_oracle": acc},
             "forms_patches_per_s": forms,
             "metric_by_form": by_form,
-            "extra_workloads": {"batch64_uneven": batch},
+            "extra_workloads": {"batch64_uneven": batch, "img4096_p16s2_k512": big},
             "clocks": clk_summary,
         }
         if cpu:

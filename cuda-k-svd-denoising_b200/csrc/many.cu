@@ -209,10 +209,8 @@ extern "C" ksvd_status ksvd_denoise_many(const ksvd_image_job* jobs, int count, 
       cudaGetLastError();
       return KSVD_ERR_CUDA;
     }
-    cudaEvent_t dn = new_event();
-    if (cudaEventRecord(dn, main_s) != cudaSuccess) return KSVD_ERR_CUDA;
-    for (auto s : pool)
-      if (cudaStreamWaitEvent(s, dn, 0) != cudaSuccess) return KSVD_ERR_CUDA;
+    // the pool streams are joined into the main stream here; whatever runs
+    // on them next starts with a fork from the main stream
     return KSVD_OK;
   };
 
