@@ -11,7 +11,9 @@
 //     each OMP step streams those blocks through a ring of shared-memory
 //     slots with 1-D bulk copies (thread 0 issues both the copies and the
 //     MMAs; a slot is refilled once the MMA that read it has committed);
-//   * the accumulator takes up to 512 TMEM columns (M = 128 patches, N = Kp);
+//   * the accumulator takes up to 512 TMEM columns (M = 128 patches, N = Kp,
+//     as up to two MMAs per K-slice: UMMA N is at most 256 with M = 128;
+//     atoms 256.. go to TMEM columns 256..);
 //     the epilogue reads each thread's quarter of the columns twice (largest
 //     |c| first, then the candidates inside the error window) instead of
 //     holding it in registers;
@@ -201,7 +203,10 @@ __global__ void __launch_bounds__(kTbThreads, 1)
   __syncthreads();
   tc_fence_after();
   const unsigned tmem = *tmem_slot;
-  const unsigned idesc = umma_idesc_16(kTbTile, Kp, TbOp<F16>::fmt);
+  // atoms [0, n0) and [256, 256 + n1): one MMA each per K-slice (N <= 256)
+  const int n0 = Kp < 256 ? Kp : 256, n1 = Kp - n0;
+  const unsigned idesc0 = umma_idesc_16(kTbTile, n0, TbOp<F16>::fmt);
+  const unsigned idesc1 = umma_idesc_16(kTbTile, n1 > 0 ? n1 : 16, TbOp<F16>::fmt);
   const unsigned a_base = smem_u32(At);
   // ring bookkeeping (thread 0 only): slices issued / consumed over the
   // kernel's life; slice i uses slot i % kTbSlots
@@ -248,8 +253,10 @@ __global__ void __launch_bounds__(kTbThreads, 1)
       full_par ^= 1u << s;
       tc_fence_after();
       const unsigned long long ad = umma_desc(a_base + kk * 2 * kTbTile * 16, kTbTile * 16, 128);
-      const unsigned long long bd = umma_desc(smem_u32(ring + size_t(s) * lo.slot_bytes), Kp * 16, 128);
-      tc_mma(tmem, ad, bd, idesc, kk > 0 ? 1u : 0u);
+      const unsigned slot = smem_u32(ring + size_t(s) * lo.slot_bytes);
+      // rows 256.. of the slice start 256 / 8 core matrices (of 128 bytes) in
+      tc_mma(tmem, ad, umma_desc(slot, Kp * 16, 128), idesc0, kk > 0 ? 1u : 0u);
+      if (n1 > 0) tc_mma(tmem + 256u, ad, umma_desc(slot + (256 / 8) * 128, Kp * 16, 128), idesc1, kk > 0 ? 1u : 0u);
       tc_commit(empty + s);
       empty_pending |= 1u << s;
       ++consumed;
