@@ -347,7 +347,8 @@ cudaError_t launch_gemm(const GemmArgs& g, bool a_kcontig, bool b_kcontig, int e
 // Elementwise kernels of the proposal
 // ---------------------------------------------------------------------------
 
-// Network input: x = y * sqrt(n) / |y| (0 for a zero patch) as BF16, padded
+// Network input: the patch with its mean removed, scaled to norm sqrt(n),
+// x = (y - mean) sqrt(n) / |y - mean| (0 for a flat patch), as BF16, padded
 // with zeros to np16 columns.  rows (optional) selects the patches: patch
 // rows[b] mod `mod` (mod 0: rows[b]).
 __global__ void mlp_input_kernel(const float* __restrict__ Y, int64_t B, int n, int np16,
@@ -357,11 +358,15 @@ __global__ void mlp_input_kernel(const float* __restrict__ Y, int64_t B, int n, 
   for (int64_t b = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); b < B; b += warps) {
     const int64_t p = rows ? (mod > 0 ? rows[b] % mod : rows[b]) : b;
     const float* y = Y + p * n;
+    float sm = 0.0f;
+    for (int k = lane; k < n; k += 32) sm += y[k];
+    const float mean = warp_sum(sm) / float(n);
     float ss = 0.0f;
-    for (int k = lane; k < n; k += 32) ss = fmaf(y[k], y[k], ss);
+    for (int k = lane; k < n; k += 32) ss = fmaf(y[k] - mean, y[k] - mean, ss);
     ss = warp_sum(ss);
     const float sc = ss > 0.0f ? sqrtf(float(n) / ss) : 0.0f;
-    for (int k = lane; k < np16; k += 32) X[b * np16 + k] = __float2bfloat16_rn(k < n ? y[k] * sc : 0.0f);
+    for (int k = lane; k < np16; k += 32)
+      X[b * np16 + k] = __float2bfloat16_rn(k < n ? (y[k] - mean) * sc : 0.0f);
   }
 }
 

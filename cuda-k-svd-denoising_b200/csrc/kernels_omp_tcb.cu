@@ -35,7 +35,7 @@ constexpr int kTbThreads = kTbTile * kTbQ;
 constexpr int kTbSlots = 4;   // ring of K-slices
 constexpr int kTbLMax = 16;
 constexpr int kTbMaxK = 512;
-constexpr int kTbMaxN = 256;
+constexpr int kTbMaxN = 512;
 constexpr unsigned long long kTbWaitNs = 2000000000ull;
 constexpr float kTbErrBf16 = 2.0f / 256.0f + 4.0e-4f;
 constexpr float kTbErrF16 = 2.0f / 2048.0f + 1.0e-4f;

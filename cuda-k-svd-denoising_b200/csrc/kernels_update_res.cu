@@ -50,7 +50,7 @@ __host__ __device__ inline int ur_n4(int n) { return (n + 3) & ~3; }
 __host__ __device__ inline int ur_es(int n) { return 4 * ((ur_n4(n) / 4) | 1); }
 constexpr int kUrRows = 32;  // reduction rows: 16 column groups + 16 streaming warps
 
-// Shared memory: [cap x es] columns | ent[2][cap] | xold[2][cap] | keep[cap] |
+// Shared memory: [cap x es] columns | ent[2][cap] | xold[2][cap] | keep[2][cap] |
 // u[n4] | dold[n4] | dnext[n4] | wred[kUrRows x n4]
 __host__ __device__ inline size_t ur_fixed_bytes(int n) {
   const int n4 = ur_n4(n);
@@ -58,14 +58,14 @@ __host__ __device__ inline size_t ur_fixed_bytes(int n) {
 }
 
 int update_res_capacity(int n) {
-  const size_t per = size_t(ur_es(n)) * 4 + 20;
+  const size_t per = size_t(ur_es(n)) * 4 + 24;
   const size_t fixed = ur_fixed_bytes(n);
   if (fixed + per * 16 > kUrSmemMax) return 0;
   // a multiple of 4 keeps u, dold, dnext and wred (read as float4) 16-byte aligned
   return int((kUrSmemMax - fixed) / per) & ~3;
 }
 
-size_t update_res_smem_bytes(int n, int cap) { return size_t(cap) * (size_t(ur_es(n)) * 4 + 20) + ur_fixed_bytes(n); }
+size_t update_res_smem_bytes(int n, int cap) { return size_t(cap) * (size_t(ur_es(n)) * 4 + 24) + ur_fixed_bytes(n); }
 
 // Bounded spin of thread 0 until *ctr >= target.  False on timeout or when an
 // error is already flagged.
@@ -196,8 +196,8 @@ __global__ void __launch_bounds__(kUrThreads, 1)
   const float4* Es4 = reinterpret_cast<const float4*>(ursm);
   int* ent_b = reinterpret_cast<int*>(ursm + size_t(cap) * es * 4);  // [2][cap]
   float* xold_b = reinterpret_cast<float*>(ent_b + 2 * cap);           // [2][cap]
-  int* keep = reinterpret_cast<int*>(xold_b + 2 * cap);  // residual row stored back (per resident column)
-  float* u = reinterpret_cast<float*>(keep + cap);
+  int* keep_b = reinterpret_cast<int*>(xold_b + 2 * cap);  // [2][cap]: residual row stored back
+  float* u = reinterpret_cast<float*>(keep_b + 2 * cap);
   float* dold = u + n4;
   float* dnext = dold + n4;
   float* wred = dnext + n4;  // [kUrRows][n4]
@@ -253,11 +253,14 @@ __global__ void __launch_bounds__(kUrThreads, 1)
     sb = int(int64_t(c) * b / active);
     se = int(int64_t(c) * (b + 1) / active);
   };
-  // entries and old coefficients of [sb, sb + cnt) into meta buffer `slot`
-  // and atom a into dst (all threads; several loads in flight per thread)
+  // entries, old coefficients and store-back flags of [sb, sb + cnt) into
+  // meta buffer `slot` and atom a into dst (all threads; several loads in
+  // flight per thread).  A residual row is stored back unless a is the last
+  // atom of the patch's support.
   auto load_meta = [&](int beg, int sb, int cnt, int slot, int a, float* dst) {
     int* ent = ent_b + slot * cap;
     float* xo = xold_b + slot * cap;
+    int* kp = keep_b + slot * cap;
     constexpr int kB = 4;
     for (int t0 = tid; t0 < cnt; t0 += kUrThreads * kB) {
       int e[kB];
@@ -267,14 +270,20 @@ __global__ void __launch_bounds__(kUrThreads, 1)
         e[k] = (t < cnt) ? __ldg(entries + beg + sb + t) : 0;
       }
       float x[kB];
+      int lt[kB];
 #pragma unroll
-      for (int k = 0; k < kB; ++k) x[k] = (t0 + k * kUrThreads < cnt) ? __ldcg(coef + e[k]) : 0.0f;
+      for (int k = 0; k < kB; ++k) {
+        const bool in = t0 + k * kUrThreads < cnt;
+        x[k] = in ? __ldcg(coef + e[k]) : 0.0f;
+        lt[k] = (in && last != nullptr) ? __ldg(last + e[k] / L) : -1;
+      }
 #pragma unroll
       for (int k = 0; k < kB; ++k) {
         const int t = t0 + k * kUrThreads;
         if (t < cnt) {
           ent[t] = e[k];
           xo[t] = x[k];
+          kp[t] = (lt[k] != a) ? 1 : 0;
         }
       }
     }
@@ -317,6 +326,7 @@ __global__ void __launch_bounds__(kUrThreads, 1)
     const int* ent_s = ent_b + slot * cap;
     const float* xold_s = xold_b + slot * cap;
     float* v_s = xold_b + slot * cap;  // per-column scalars once the columns are built
+    const int* keep_s = keep_b + slot * cap;
 
     // ---- entries, old coefficients and the old atom: never written by other
     // atoms, so read before the wait (or prefetched during the previous atom)
@@ -609,7 +619,6 @@ __global__ void __launch_bounds__(kUrThreads, 1)
       const float x = (q < mc) ? dot_u(q) : 0.0f;
       v_s[q] = x;
       __stcg(coef + ent_s[q], x);
-      keep[q] = (last == nullptr || __ldg(last + ent_s[q] / L) != j) ? 1 : 0;
     }
     if (m > cap) {  // streamed columns: a warp per two columns
       float ur[NW];
@@ -661,7 +670,7 @@ __global__ void __launch_bounds__(kUrThreads, 1)
     if (tma) {  // rows of 16-byte aligned float4
       for (int t = tid; t < mres * F; t += kUrThreads) {
         const int q = t / F, f = t - q * F;
-        if (!keep[q]) continue;
+        if (!keep_s[q]) continue;
         const float x = v_s[q];
         const float4 e = Es4[size_t(q) * es4 + f], w = u4[f];
         float4 r;
@@ -674,7 +683,7 @@ __global__ void __launch_bounds__(kUrThreads, 1)
     } else {
       for (int t = tid; t < mres * n; t += kUrThreads) {
         const int q = t / n, i = t - q * n;
-        if (keep[q]) __stcg(R + int64_t(ent_s[q] / L) * n + i, fmaf(-v_s[q], u[i], Es[size_t(q) * es + i]));
+        if (keep_s[q]) __stcg(R + int64_t(ent_s[q] / L) * n + i, fmaf(-v_s[q], u[i], Es[size_t(q) * es + i]));
       }
     }
     fence_proxy_async_smem();  // generic accesses of Es before the next bulk copies into it

@@ -316,7 +316,7 @@ ksvd_status ksvd_set_update_slice(ksvd_ctx* ctx, int slice);
  * full OMP.  The reference has no counterpart: its OMP scores every atom
  * (cublas_matrix_omp.cu:193-233).
  *
- * Network: x = y sqrt(n) / |y|  ->  512 (GELU)  ->  512 (GELU)  ->  atoms
+ * Network: x = (y - mean) sqrt(n) / |y - mean|  ->  512 (GELU)  ->  512 (GELU)  ->  atoms
  * (sigmoid scores); BF16 weights and activations, FP32 accumulation, FP32
  * master weights trained with Adam on the binary cross-entropy between the
  * scores and the support mask.  Parameters, in this order, row-major:

@@ -2,7 +2,8 @@
 checker for tests/; the product library never imports it).
 
 The network of the library's learned OMP form (include/ksvd_sm100.h,
-"learned support proposal"): x = y sqrt(n) / |y|, two hidden layers of 512
+"learned support proposal"): x = (y - mean) sqrt(n) / |y - mean|, two hidden
+layers of 512
 GELU units, one score per atom, binary cross-entropy between the sigmoid
 scores and the OMP support mask, mean over the B x K entries.  Parameters in
 the library's order: W1 [512 x n], b1, W2 [512 x 512], b2, W3 [K x 512], b3.
@@ -52,12 +53,14 @@ def unpack(params: np.ndarray, n: int, K: int):
 
 
 def inputs(Y: np.ndarray) -> np.ndarray:
-    """x = y sqrt(n) / |y| in FP32 (0 for a zero patch), as float64."""
+    """x = (y - mean) sqrt(n) / |y - mean| in FP32 (0 for a flat patch), as
+    float64."""
     Y = np.asarray(Y, np.float32)
     n = Y.shape[1]
-    ss = np.sum(Y.astype(np.float64) ** 2, axis=1)
+    C = (Y - Y.mean(axis=1, dtype=np.float64)[:, None].astype(np.float32)).astype(np.float32)
+    ss = np.sum(C.astype(np.float64) ** 2, axis=1)
     sc = np.where(ss > 0, np.sqrt(n / np.where(ss > 0, ss, 1.0)), 0.0).astype(np.float32)
-    return (Y * sc[:, None]).astype(np.float64)
+    return (C * sc[:, None]).astype(np.float64)
 
 
 def gelu(z):

@@ -51,13 +51,16 @@ def test_omp_512_atoms_16x16(torch_cuda, ksvd, oracle, synth, precision):
     check_omp(idx, coef, ri, rc)
 
 
-def test_omp_22x22_patches(torch_cuda, ksvd, oracle, synth):
-    """n = 484 (22x22 patches), K = 256, L = 5."""
+@pytest.mark.parametrize("precision", [0, 2])
+def test_omp_22x22_patches(torch_cuda, ksvd, oracle, synth, precision):
+    """n = 484 (22x22 patches), K = 256, L = 5: FP32 with the dictionary
+    streamed through shared memory, FP16 with the 16-bit dictionary streamed
+    slice by slice (kernels_omp_tcb.cu)."""
     noisy = synth.add_gaussian(synth.clean_image(112, 42), 25.0, 42)
     Y = oracle.extract_patches(noisy, 22, 22, 3, 3)
     D = oracle.init_dictionary(Y, 256, int_norm=True, dtype=np.float32)
     idx, coef = run_omp(torch_cuda, ksvd, Y, D, patch_width_dim=22, patch_height_dim=22, sliding_width=3,
-                        sliding_height=3, atoms=256, omp_iter=5)
+                        sliding_height=3, atoms=256, omp_iter=5, precision=precision)
     ri, rc = oracle.omp(Y.astype(np.float64), D.astype(np.float64), 5)
     check_omp(idx, coef, ri, rc)
 
