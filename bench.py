@@ -232,7 +232,7 @@ def quality_vs_fp64(pkg, oracle, wl, clean, noisy, D0, patches, make_ctx, forms)
     return res
 
 
-def batch_workload(pkg, ksvd, count=64, tune=True):
+def batch_workload(pkg, ksvd, count=64, tune=False):
     """The uneven batch (64 seeded images, sides 256..2048, patches 8/12/22
     at stride 3, 16 speckle): ksvd_denoise_many end to end (host images in
     and out), beside the same images denoised one by one with ksvd_denoise in
@@ -253,9 +253,11 @@ def batch_workload(pkg, ksvd, count=64, tune=True):
     outs, st = ksvd.denoise_many(specs, tune=tune)
     wall_batch = time.perf_counter() - t
     t = time.perf_counter()
+    seq_iter_ms = 0.0
     for prm, img, s2 in specs:
         with ksvd.Context(prm) as c:
-            c.denoise(img, s2)
+            _, sst = c.denoise(img, s2)
+            seq_iter_ms += sst["iter_ms"]
     wall_seq = time.perf_counter() - t
     T = jobs[0]["ksvd_iter"]
     psnr_gain = [pkg.synth.psnr(j["clean"], o) - pkg.synth.psnr(j["clean"], j["noisy"]) for j, o in zip(jobs, outs)]
@@ -264,7 +266,9 @@ def batch_workload(pkg, ksvd, count=64, tune=True):
             "speckle_images": sum(j["speckle"] for j in jobs),
             "iter_patches_per_s": st["num_patches"] * T / (st["iter_ms"] / 1000.0),
             "iter_ms": st["iter_ms"], "call_device_ms": st["total_ms"], "call_wall_s": wall_batch,
-            "sequential_wall_s": wall_seq, "speedup_vs_one_by_one": wall_seq / wall_batch,
+            "setup_ms": st["setup_ms"], "tune_ms": st["tune_ms"], "final_ms": st["final_ms"],
+            "one_by_one_iter_ms": seq_iter_ms, "iter_speedup_vs_one_by_one": seq_iter_ms / st["iter_ms"],
+            "one_by_one_wall_s": wall_seq, "wall_speedup_vs_one_by_one": wall_seq / wall_batch,
             "graph": st["graph"], "streams": st["streams"], "split_alpha": st["split_alpha"],
             "update_ctas_min_max": [min(st["update_ctas"]), max(st["update_ctas"])],
             "psnr_gain_db_min_median": [float(np.min(psnr_gain)), float(np.median(psnr_gain))],
@@ -538,6 +542,12 @@ def main():
         torch.cuda.synchronize()
         if i > 0:  # first call is a warm-up
             e2e_ms.append(e0.elapsed_time(e1))
+    # one more call with per-family timing: the gather and the rebuild
+    ctx.profile(1)
+    ctx.profile_reset()
+    ctx.denoise_ptr(img_h.data_ptr(), W, H, sigma2, out_h.data_ptr())
+    img_fams = {f: ctx.profile_read(f) for f in ("im2col", "col2im", "blend")}
+    ctx.profile(0)
     e2e_call_ms = float(np.median(e2e_ms))
     e2e_call_ms = reduce_max(e2e_call_ms, dist, "cuda")
     e2e_value = aggregate_rate(N * wl.ksvd_iter, world, e2e_call_ms)
@@ -585,6 +595,16 @@ def main():
                 tfs = flops_pp * N / (ms_f / 1000.0) / 1e12
                 per_kernel[f].update({"flops_per_patch": flops_pp, "achieved_tflops": tfs,
                                       "frac_tensor": tfs / peak_tc})
+        # the patch gather and the image rebuild (per call of ksvd_denoise):
+        #   im2col: write the patches (4n per patch) + read the image (4 per pixel)
+        #   col2im: read the codes (8L per patch) + read the noisy image and
+        #           write the overlap sums (8 per pixel); the dictionary is L2-resident
+        for f, nbytes in (("im2col", 4 * n * N + 4 * W * H), ("col2im", 8 * L * N + 8 * W * H)):
+            ms_f = img_fams[f][0]
+            if ms_f > 0:
+                gbs = nbytes / (ms_f / 1000.0) / 1e9
+                per_kernel[f] = {"ms_per_call": ms_f, "bytes_per_call": nbytes, "achieved_gbs": gbs,
+                                 "frac_hbm": gbs / peak}
         # the whole iteration against max(F / tensor peak, B / HBM peak) with
         # the compulsory bytes B = 4n + 8L (OMP) + L(4n + 8) + 4L (update)
         b_iter = 4 * n + 8 * L + L * (4 * n + 8) + 4 * L

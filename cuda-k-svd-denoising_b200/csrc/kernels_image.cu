@@ -2,7 +2,9 @@
 //
 // The reference forms all denoised patches D X with one SGEMM, copies them to
 // the host and overlap-adds them in a single host thread.  Here:
-//   col2im_kernel  one CTA per TS x TS pixel tile: the denoised patches that
+//   col2im_kernel  one CTA per TS x TS pixel tile (TS = 32, 16 or 8; large
+//                  patches use col2im_direct_kernel, one thread per pixel,
+//                  with the same sums): the denoised patches that
 //                  cover the tile (x_hat_p = sum_s x_s d_s from the compact
 //                  codes) are formed in shared memory, then each pixel sums
 //                  the covering patches in patch order (ix, then iy, the
@@ -24,17 +26,23 @@ constexpr size_t kCol2imSmemLimit = 100 * 1024;
 
 static int tile_patches_1d(int TS, int ext, int stride) { return (TS + ext - 1) / stride + 1; }
 
+// Tile side of the shared-memory gather: the largest of 32, 16, 8 whose
+// covering patches fit the budget; 0 when none does (large patches), in
+// which case the direct gather runs.
 static int pick_tile(const PatchGeom& g) {
-  const int cands[] = {32, 16, 8, 4, 2, 1};
+  const int cands[] = {32, 16, 8};
   for (int TS : cands) {
     size_t np = size_t(tile_patches_1d(TS, g.ph, g.sh)) * tile_patches_1d(TS, g.pw, g.sw);
     if (np * g.n * sizeof(float) <= kCol2imSmemLimit) return TS;
   }
-  return 1;
+  return 0;
 }
 
+constexpr int kDirectThreads = 256;
+
 int col2im_num_tiles(const PatchGeom& g) {
-  int TS = pick_tile(g);
+  const int TS = pick_tile(g);
+  if (TS == 0) return int((int64_t(g.W) * g.H + kDirectThreads - 1) / kDirectThreads);
   return ((g.W + TS - 1) / TS) * ((g.H + TS - 1) / TS);
 }
 
@@ -60,14 +68,23 @@ __global__ void __launch_bounds__(256) col2im_kernel(const float* __restrict__ n
   for (int q = warp; q < npx * npy; q += nwarps) {
     const int ix = ixl + q / npy, iy = iyl + q % npy;
     const int64_t p = int64_t(ix) * g.ny + iy;
-    for (int i = lane; i < g.n; i += 32) {
+    // the patch's code, one (atom, coefficient) pair per lane, broadcast below
+    int a_l = -1;
+    float x_l = 0.0f;
+    if (lane < L) {
+      a_l = __ldg(idx + p * L + lane);
+      x_l = __ldg(coef + p * L + lane);
+      if (a_l < 0 || a_l >= K) a_l = -1;
+    }
+    for (int i0 = 0; i0 < g.n; i0 += 32) {
+      const int i = i0 + lane;
       float v = 0.0f;
-      for (int s = 0; s < L; ++s) {
-        const int a = __ldg(idx + p * L + s);
-        if (a < 0 || a >= K) continue;
-        v = fmaf(__ldg(coef + p * L + s), __ldg(D + int64_t(a) * g.n + i), v);
+      for (int s = 0; s < L; ++s) {  // L <= 32, the same trip count in every lane
+        const int a = __shfl_sync(0xffffffffu, a_l, s);
+        const float x = __shfl_sync(0xffffffffu, x_l, s);
+        if (a >= 0 && i < g.n) v = fmaf(x, __ldg(D + int64_t(a) * g.n + i), v);
       }
-      xs[q * g.n + i] = v;
+      if (i < g.n) xs[q * g.n + i] = v;
     }
   }
   __syncthreads();
@@ -93,6 +110,48 @@ __global__ void __launch_bounds__(256) col2im_kernel(const float* __restrict__ n
   }
   part = block_sum(part, red);
   if (threadIdx.x == 0) partials[blockIdx.y * gridDim.x + blockIdx.x] = part;
+}
+
+// The same sums without shared memory, for patches too large for a tile's
+// covering patches to fit it: one thread per pixel forms the element of each
+// covering patch it needs (x_hat_p[r] = sum_s x_s d_s[r], the same FMA order
+// as col2im_kernel) and adds them in the same patch order, so the result is
+// identical; each block reduces its share of the lambda sum.
+__global__ void __launch_bounds__(kDirectThreads) col2im_direct_kernel(
+    const float* __restrict__ noisy, PatchGeom g, const float* __restrict__ D, int K, int L,
+    const int32_t* __restrict__ idx, const float* __restrict__ coef, float* __restrict__ acc_out,
+    double* __restrict__ partials) {
+  __shared__ double red[32];
+  const int64_t P = int64_t(g.W) * g.H;
+  const int64_t q = int64_t(blockIdx.x) * kDirectThreads + threadIdx.x;
+  double part = 0.0;
+  if (q < P) {
+    const int y = int(q / g.W), x = int(q - int64_t(y) * g.W);
+    const int ia = cover_lo(x, g.ph, g.sh), ib = cover_hi(x, g.sh, g.nx);
+    const int ja = cover_lo(y, g.pw, g.sw), jb = cover_hi(y, g.sw, g.ny);
+    float acc = 0.0f;
+    int w = 0;
+    for (int ix = ia; ix <= ib; ++ix)
+      for (int iy = ja; iy <= jb; ++iy) {
+        const int64_t p = int64_t(ix) * g.ny + iy;
+        const int off = (x - ix * g.sh) * g.pw + (y - iy * g.sw);
+        float v = 0.0f;
+        for (int s = 0; s < L; ++s) {
+          const int a = __ldg(idx + p * L + s);
+          if (a < 0 || a >= K) continue;
+          v = fmaf(__ldg(coef + p * L + s), __ldg(D + int64_t(a) * g.n + off), v);
+        }
+        acc += v;
+        ++w;
+      }
+    acc_out[q] = acc;
+    if (w > 0) {
+      const double d = double(acc) / double(w) - double(noisy[q]);
+      part = d * d;
+    }
+  }
+  part = block_sum(part, red);
+  if (threadIdx.x == 0) partials[blockIdx.x] = part;
 }
 
 __global__ void __launch_bounds__(1024) lambda_kernel(const double* __restrict__ partials, int np, double sigma2,
@@ -125,6 +184,12 @@ cudaError_t launch_col2im(const float* noisy, const PatchGeom& g, const float* d
                           const int32_t* idx, const float* coef, float* acc, double* partials, int* num_partials,
                           cudaStream_t s) {
   const int TS = pick_tile(g);
+  if (TS == 0) {
+    const int64_t blocks = (int64_t(g.W) * g.H + kDirectThreads - 1) / kDirectThreads;
+    col2im_direct_kernel<<<unsigned(blocks), kDirectThreads, 0, s>>>(noisy, g, dict, K, L, idx, coef, acc, partials);
+    *num_partials = int(blocks);
+    return cudaGetLastError();
+  }
   const size_t np = size_t(tile_patches_1d(TS, g.ph, g.sh)) * tile_patches_1d(TS, g.pw, g.sw);
   const size_t smem = np * g.n * sizeof(float);
   if (smem > 48 * 1024) {

@@ -123,8 +123,8 @@ extern "C" ksvd_status ksvd_denoise_many(const ksvd_image_job* jobs, int count, 
 
   MANY_CU(cudaStreamCreateWithFlags(&main_s, cudaStreamNonBlocking));
   for (auto& s : pool) MANY_CU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-  cudaEvent_t t0 = nullptr, t1 = nullptr, t2 = nullptr, t3 = nullptr;
-  for (cudaEvent_t* e : {&t0, &t1, &t2, &t3}) {
+  cudaEvent_t t0 = nullptr, t1 = nullptr, t2 = nullptr, t3 = nullptr, ts = nullptr, ti = nullptr;
+  for (cudaEvent_t* e : {&t0, &t1, &t2, &t3, &ts, &ti}) {
     MANY_CU(cudaEventCreate(e));
     evs.push_back(*e);
   }
@@ -214,6 +214,7 @@ extern "C" ksvd_status ksvd_denoise_many(const ksvd_image_job* jobs, int count, 
     return KSVD_OK;
   };
 
+  MANY_CU(cudaEventRecord(ts, main_s));  // set-up done (the init calls synchronised every image's stream)
   MANY_CU(cudaEventRecord(t1, main_s));
   int used_graph = 0;
   if (T > 0) {
@@ -295,6 +296,7 @@ extern "C" ksvd_status ksvd_denoise_many(const ksvd_image_job* jobs, int count, 
     }
   }
   MANY_CU(cudaEventRecord(t2, main_s));
+  MANY_CU(cudaEventRecord(ti, main_s));
   // ---- final OMP and the rebuild, per image ----------------------------------
   cudaEvent_t fk = new_event();
   MANY_CU(cudaEventRecord(fk, main_s));
@@ -325,6 +327,12 @@ extern "C" ksvd_status ksvd_denoise_many(const ksvd_image_job* jobs, int count, 
     stats->num_patches = total_patches;
     stats->iter_ms = a;
     stats->total_ms = b;
+    cudaEventElapsedTime(&a, t0, ts);
+    stats->setup_ms = a;
+    cudaEventElapsedTime(&a, ts, t1);
+    stats->tune_ms = a;
+    cudaEventElapsedTime(&a, ti, t3);
+    stats->final_ms = a;
     stats->graph = used_graph;
     stats->streams = S;
     stats->split_alpha = alpha;

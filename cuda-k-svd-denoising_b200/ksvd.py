@@ -120,6 +120,9 @@ class ManyStats(ctypes.Structure):
         ("streams", ctypes.c_int),
         ("split_alpha", ctypes.c_double),
         ("update_ctas", ctypes.c_int * 64),
+        ("setup_ms", ctypes.c_double),
+        ("tune_ms", ctypes.c_double),
+        ("final_ms", ctypes.c_double),
     ]
 
     def as_dict(self, count: int) -> dict:

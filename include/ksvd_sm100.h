@@ -283,6 +283,9 @@ typedef struct ksvd_many_stats {
   int streams;         /* streams in the pool */
   double split_alpha;  /* SMs split by (sweep bytes)^alpha */
   int update_ctas[64]; /* CTAs of each image in the shared sweep */
+  double setup_ms;     /* uploads, patch gathers, initial dictionaries */
+  double tune_ms;      /* choosing the SM split (0 without tuning) */
+  double final_ms;     /* final OMP, rebuild and downloads */
 } ksvd_many_stats;
 
 ksvd_status ksvd_denoise_many(const ksvd_image_job* jobs, int count, int device, int tune, ksvd_many_stats* stats);
