@@ -502,7 +502,7 @@ __global__ void __launch_bounds__(kUrThreads, 1)
         if (g < Gr) {
           float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
           const float4* base = reinterpret_cast<const float4*>(gw + size_t(it & 1) * G * n4) + f;
-          constexpr int kB = 8;
+          constexpr int kB = 12;  // one round of loads for up to 12 Gr partials per thread
           for (int bb0 = g; bb0 < active; bb0 += Gr * kB) {
             float4 v[kB];
 #pragma unroll
