@@ -13,7 +13,9 @@
 //     cublasIsamax does (:216-233);
 //   * the least-squares coefficients on the support (the reference's
 //     pseudo-inverse, :269-339) come from a Cholesky factor of the support
-//     Gram grown by one row per step, in FP64 from the FP64 dictionary Gram;
+//     Gram grown by one row per step, in FP64 from the FP64 dictionary Gram
+//     (diagonal kept inverted; the forward solution z = L^-1 b grows by one
+//     element per step, only the back substitution runs over the support);
 //   * the residual y - D_S g (:352-380) and its norm (:382-393) are formed
 //     per patch by one warp; a patch whose residual norm is below 1e-3 stops
 //     (:218).
@@ -273,7 +275,7 @@ __global__ void __launch_bounds__(kOmpThreads, 1)
           for (int i = 0; i < k; ++i) {
             double s = g[i];
             for (int j2 = 0; j2 < i; ++j2) s -= Lp[i * L + j2] * Lp[k * L + j2];
-            const double wi = s / Lp[i * L + i];
+            const double wi = s * Lp[i * L + i];  // the diagonal is kept as 1 / L_ii
             Lp[k * L + i] = wi;
             ww += wi * wi;
           }
@@ -281,20 +283,20 @@ __global__ void __launch_bounds__(kOmpThreads, 1)
           if (!(piv2 > 0.0)) {
             done[p] = 1;  // the new atom depends linearly on the support
           } else {
-            Lp[k * L + k] = sqrt(piv2);
+            const double il = 1.0 / sqrt(piv2);
+            Lp[k * L + k] = il;
             S[p * L + k] = a;
-            bvec[p * L + k] = bS[p];
+            // bvec holds the forward solution z = L^-1 b of the support so
+            // far; only its new element is computed
+            double zk = bS[p];
+            for (int j2 = 0; j2 < k; ++j2) zk -= Lp[k * L + j2] * bvec[p * L + j2];
+            bvec[p * L + k] = zk * il;
             cnt[p] = k + 1;
             double yv[kLMax];
-            for (int i = 0; i <= k; ++i) {
-              double s = bvec[p * L + i];
-              for (int j2 = 0; j2 < i; ++j2) s -= Lp[i * L + j2] * yv[j2];
-              yv[i] = s / Lp[i * L + i];
-            }
             for (int i = k; i >= 0; --i) {
-              double s = yv[i];
+              double s = bvec[p * L + i];
               for (int j2 = i + 1; j2 <= k; ++j2) s -= Lp[j2 * L + i] * yv[j2];
-              yv[i] = s / Lp[i * L + i];
+              yv[i] = s * Lp[i * L + i];
             }
             for (int i = 0; i <= k; ++i) gam[p * L + i] = float(yv[i]);
           }

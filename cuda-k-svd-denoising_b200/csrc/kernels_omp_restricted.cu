@@ -6,11 +6,14 @@
 // argmax taken over the candidates only.
 //
 // One warp per patch.  Lane pair (2c, 2c + 1) owns candidate c: it forms
-// b_c = d_c . y exactly (FP64 from the FP32 data, the two lanes sum
-// alternate features) and keeps the candidate's correlation with the
+// b_c = d_c . y exactly (FP64 from the FP32 data; the two lanes sum
+// alternate groups of four features, two FP64 chains each) and keeps the candidate's correlation with the
 // residual in the Batch-OMP form
 //     alpha_c = b_c - sum_s g_s G[c][s]          (FP64, FP64 Gram)
-// so no residual vector is ever formed.  Lane 0 extends the Cholesky factor
+// so no residual vector is ever formed.  Each candidate's Gram entries with
+// the support sit in shared memory: per step all candidate lanes load their
+// one new entry at once, and the winner's row is the Cholesky append's
+// G[new][S].  Lane 0 extends the Cholesky factor
 // of the support Gram by one row per step, keeps the forward solution
 // z = L^-1 b of the support, solves for the coefficients g and tracks
 // |r|^2 = |y|^2 - |z|^2.  A patch whose final residual norm is above the
@@ -31,12 +34,13 @@ __global__ void __launch_bounds__(kRWarps * 32)
     omp_restricted_kernel(const float* __restrict__ Y, int64_t N, int n, const float* __restrict__ D,
                           const double* __restrict__ Gram, int K, int L, const int32_t* __restrict__ cand, int C,
                           double thr2, int32_t* __restrict__ idx_out, float* __restrict__ coef_out,
-                          int64_t* __restrict__ fb_list, unsigned long long* __restrict__ fb_count) {
-  __shared__ float ys[kRWarps][kRMaxN];
+                          int64_t* __restrict__ fb_list, unsigned long long* __restrict__ fb_count, int vec4) {
+  __shared__ __align__(16) float ys[kRWarps][kRMaxN];
   __shared__ double lf[kRWarps][kRLMax * (kRLMax + 1) / 2];  // Cholesky rows, diagonal as 1 / L_ii
   __shared__ double zf[kRWarps][kRLMax];                     // forward solution L^-1 b
   __shared__ double gm[kRWarps][kRLMax];                     // coefficients
   __shared__ int sup[kRWarps][kRLMax];
+  __shared__ double gcs[kRWarps][16][kRLMax + 1];  // per candidate: G[candidate][support atom s] (padded: no bank conflicts)
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int c = lane >> 1, h = lane & 1;
   double* Lp = lf[w];
@@ -58,10 +62,35 @@ __global__ void __launch_bounds__(kRWarps * 32)
       a = cand[p * C + c];
       if (a < 0 || a >= K) a = -1;
     }
+    // b_c = d_c . y in FP64: the lane pair splits the features, several
+    // independent loads in flight per lane
     double b = 0.0;
     if (a >= 0) {
       const float* d = D + int64_t(a) * n;
-      for (int k = h; k < n; k += 2) b = fma(double(__ldg(d + k)), double(ys[w][k]), b);
+      double b0 = 0.0, b1 = 0.0;
+      if (vec4) {
+        const float4* d4 = reinterpret_cast<const float4*>(d);
+        const float4* y4 = reinterpret_cast<const float4*>(ys[w]);
+        const int n4 = n >> 2;
+        for (int f0 = h; f0 < n4; f0 += 8) {
+          float4 dv[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) dv[u] = (f0 + 2 * u < n4) ? __ldg(d4 + f0 + 2 * u) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            if (f0 + 2 * u < n4) {
+              const float4 yv = y4[f0 + 2 * u];
+              b0 = fma(double(dv[u].x), double(yv.x), b0);
+              b1 = fma(double(dv[u].y), double(yv.y), b1);
+              b0 = fma(double(dv[u].z), double(yv.z), b0);
+              b1 = fma(double(dv[u].w), double(yv.w), b1);
+            }
+          }
+        }
+      } else {
+        for (int k = h; k < n; k += 2) b0 = fma(double(__ldg(d + k)), double(ys[w][k]), b0);
+      }
+      b = b0 + b1;
     }
     b += __shfl_xor_sync(0xffffffffu, b, 1);
     double alpha = b;
@@ -81,34 +110,43 @@ __global__ void __launch_bounds__(kRWarps * 32)
         // argmax |alpha| over the candidates, lowest atom index on ties
         double key = (a >= 0 && h == 0) ? fabs(alpha) : -1.0;
         int ka = (a >= 0 && h == 0) ? a : 0x7fffffff;
+        int kc = c;  // the winner's candidate slot
         double kb = b;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
           const double k2 = __shfl_xor_sync(0xffffffffu, key, o);
           const int a2 = __shfl_xor_sync(0xffffffffu, ka, o);
+          const int c2 = __shfl_xor_sync(0xffffffffu, kc, o);
           const double b2 = __shfl_xor_sync(0xffffffffu, kb, o);
           if (k2 > key || (k2 == key && a2 < ka)) {
             key = k2;
             ka = a2;
+            kc = c2;
             kb = b2;
           }
         }
         if (key < 0.0) break;  // no candidate at all
+        const int k = cnt;
+        // each candidate's Gram entry with the new atom, loaded in parallel:
+        // the support atoms are candidates, so the winner's row of the cache
+        // holds G[new][S_i] for the Cholesky append
+        if (a >= 0 && h == 0) gcs[w][c][k] = Gram[int64_t(a) * K + ka];
+        __syncwarp();
         int stop = 0;
         if (lane == 0) {
-          const int k = cnt;
           for (int s2 = 0; s2 < k; ++s2)
             if (sup[w][s2] == ka) stop = 1;  // re-selected atom: the pursuit ends
           if (!stop) {
+            const double* gw = gcs[w][kc];
             double ww = 0.0;
             for (int i = 0; i < k; ++i) {
-              double s3 = Gram[int64_t(sup[w][i]) * K + ka];
+              double s3 = gw[i];
               for (int j = 0; j < i; ++j) s3 -= Lat(i, j) * Lat(k, j);
               const double wi = s3 * Lat(i, i);
               Lat(k, i) = wi;
               ww += wi * wi;
             }
-            const double piv2 = Gram[int64_t(ka) * K + ka] - ww;
+            const double piv2 = gw[k] - ww;
             if (!(piv2 > 0.0)) {
               stop = 1;  // the new atom depends linearly on the support
             } else {
@@ -134,9 +172,9 @@ __global__ void __launch_bounds__(kRWarps * 32)
         double zz = 0.0;
         for (int i = 0; i < cnt; ++i) zz = fma(zf[w][i], zf[w][i], zz);
         rr = yy - zz;
-        if (a >= 0) {
+        if (a >= 0 && h == 0) {
           double s3 = b;
-          for (int i = 0; i < cnt; ++i) s3 = fma(-gm[w][i], Gram[int64_t(a) * K + sup[w][i]], s3);
+          for (int i = 0; i < cnt; ++i) s3 = fma(-gm[w][i], gcs[w][c][i], s3);
           alpha = s3;
         }
       }
@@ -185,8 +223,9 @@ cudaError_t launch_omp_restricted(const float* patches, int64_t N, int n, const 
   const int64_t want = (N + kRWarps - 1) / kRWarps;
   const int64_t cap = int64_t(num_sms) * 8;
   const int blocks = int(want < cap ? want : cap);
+  const int vec4 = ((n & 3) == 0 && (reinterpret_cast<uintptr_t>(dict) & 15) == 0) ? 1 : 0;
   omp_restricted_kernel<<<blocks > 0 ? blocks : 1, kRWarps * 32, 0, s>>>(patches, N, n, dict, gram, K, L, cand, C,
-                                                                          thr2, idx, coef, fb_list, fb_count);
+                                                                          thr2, idx, coef, fb_list, fb_count, vec4);
   return cudaGetLastError();
 }
 

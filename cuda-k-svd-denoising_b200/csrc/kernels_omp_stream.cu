@@ -341,7 +341,7 @@ __global__ void __launch_bounds__(kSThreads, 1)
           for (int i = 0; i < k; ++i) {
             double s = g[i];
             for (int j2 = 0; j2 < i; ++j2) s -= Lp[i * L + j2] * Lp[k * L + j2];
-            const double wi = s / Lp[i * L + i];
+            const double wi = s * Lp[i * L + i];  // the diagonal is kept as 1 / L_ii
             Lp[k * L + i] = wi;
             ww += wi * wi;
           }
@@ -349,20 +349,20 @@ __global__ void __launch_bounds__(kSThreads, 1)
           if (!(piv2 > 0.0)) {
             done[p] = 1;  // the new atom depends linearly on the support
           } else {
-            Lp[k * L + k] = sqrt(piv2);
+            const double il = 1.0 / sqrt(piv2);
+            Lp[k * L + k] = il;
             S[p * L + k] = a;
-            bvec[p * L + k] = bS[p];
+            // bvec holds the forward solution z = L^-1 b of the support so
+            // far; only its new element is computed
+            double zk = bS[p];
+            for (int j2 = 0; j2 < k; ++j2) zk -= Lp[k * L + j2] * bvec[p * L + j2];
+            bvec[p * L + k] = zk * il;
             cnt[p] = k + 1;
             double yv[kSLMax];
-            for (int i = 0; i <= k; ++i) {
-              double s = bvec[p * L + i];
-              for (int j2 = 0; j2 < i; ++j2) s -= Lp[i * L + j2] * yv[j2];
-              yv[i] = s / Lp[i * L + i];
-            }
             for (int i = k; i >= 0; --i) {
-              double s = yv[i];
+              double s = bvec[p * L + i];
               for (int j2 = i + 1; j2 <= k; ++j2) s -= Lp[j2 * L + i] * yv[j2];
-              yv[i] = s / Lp[i * L + i];
+              yv[i] = s * Lp[i * L + i];
             }
             for (int i = 0; i <= k; ++i) gam[p * L + i] = float(yv[i]);
           }
