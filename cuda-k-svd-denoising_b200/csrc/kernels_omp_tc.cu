@@ -7,13 +7,14 @@
 //   * each OMP step, one thread issues n/16 tcgen05.mma (M = 128 patches,
 //     N = atoms, K = 16, BF16 inputs, FP32 accumulation in tensor memory) and
 //     commits them to an mbarrier;
-//   * thread m of the 128 epilogue threads owns TMEM lane m = patch m: it
-//     streams its row of correlations out of tensor memory (tcgen05.ld),
-//     keeps the kTopT largest |c|, re-scores those candidates exactly,
+//   * the four threads of patch m own TMEM lane m and a quarter of its
+//     columns each: they stream the correlations out of tensor memory
+//     (tcgen05.ld), keep the atoms inside the 16-bit error window, and the
+//     CTA re-scores every windowed candidate exactly,
 //         c_a = d_a . y - sum_s g_s <d_a, d_s>   (FP64, FP32 inputs)
-//     and takes the largest, lowest atom index on ties (cublasIsamax,
+//     taking the largest, lowest atom index on ties (cublasIsamax,
 //     :216-233);
-//   * it extends the Cholesky factor of its support Gram (FP64, from the FP64
+//   * thread (m, 0) extends the Cholesky factor of the support Gram (FP64, from the FP64
 //     dictionary Gram), solves for the coefficients (the reference's
 //     pseudo-inverse, :269-339), forms the FP32 residual y - D_S g and its
 //     norm (:352-393; stop when below 1e-3, :218) and writes the residual as
