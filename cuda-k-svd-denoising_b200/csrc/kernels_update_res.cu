@@ -172,52 +172,20 @@ KSVD_DEV void red_release_add(unsigned* p, unsigned v) {
 
 // One launch sweeps one or several problems (images): group g owns the CTAs
 // [cta_begin, cta_begin + ctas) and walks its own atoms with its own buffers,
-// counters and partials; groups never wait on one another.
+// counters and partials.  Groups whose ranges share CTAs run one after the
+// other on those CTAs, in the order of the table; a group only waits for its
+// own CTAs, and every CTA takes its groups in the same (table) order, so the
+// lowest unfinished group always has all its CTAs and the launch cannot
+// deadlock.
 template <int NW>
 __global__ void __launch_bounds__(kUrThreads, 1)
     update_res_kernel(const UpdBatch batch, GridBarrier* flags, DevStats* stats, int timers) {
   extern __shared__ __align__(16) unsigned char ursm[];
-  int gi = 0;
-  while (gi + 1 < batch.ngroups && int(blockIdx.x) >= batch.g[gi + 1].cta_begin) ++gi;
-  const UpdGroup& grp = batch.g[gi];
-  float* const R = grp.R;
-  float* const D = grp.D;
-  float* const coef = grp.coef;
-  const int* __restrict__ const atom_ptr = grp.atom_ptr;
-  const int* __restrict__ const entries = grp.entries;
-  const int* __restrict__ const last = grp.last;
-  float* const gw = grp.gw;
-  unsigned* const sync = grp.sync;
-  const int n = grp.n, K = grp.K, L = grp.L, q1_cap = grp.q1_cap, cap = grp.cap;
-  const int slice_target = grp.slice_target > 0 ? grp.slice_target : kUrDefaultSlice;
-  const int n4 = ur_n4(n), es = ur_es(n);
-  const int F = n4 / 4, es4 = es / 4;  // float4 per row of u / w, per resident column
-  float* Es = reinterpret_cast<float*>(ursm);
-  const float4* Es4 = reinterpret_cast<const float4*>(ursm);
-  int* ent_b = reinterpret_cast<int*>(ursm + size_t(cap) * es * 4);  // [2][cap]
-  float* xold_b = reinterpret_cast<float*>(ent_b + 2 * cap);           // [2][cap]
-  int* keep_b = reinterpret_cast<int*>(xold_b + 2 * cap);  // [2][cap]: residual row stored back
-  float* u = reinterpret_cast<float*>(keep_b + 2 * cap);
-  float* dold = u + n4;
-  float* dnext = dold + n4;
-  float* wred = dnext + n4;  // [kUrRows][n4]
-  float4* u4 = reinterpret_cast<float4*>(u);
-  const float4* dold4 = reinterpret_cast<const float4*>(dold);
-  float4* wred4 = reinterpret_cast<float4*>(wred);
   __shared__ int s_ok;
   __shared__ int s_stop;
   __shared__ __align__(8) unsigned long long s_mbar;  // completion of the residual-row bulk copies
   __shared__ unsigned long long s_ph[8];  // phase times of this CTA (slots 0..7)
-
-  const int G = grp.ctas, b = int(blockIdx.x) - grp.cta_begin;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  unsigned* iter_cnt = sync;
-  unsigned* done_cnt = sync + K;
-  int Gr = kUrThreads / F;  // column groups of the w pass, partial groups of the all-reduce
-  if (Gr > 16) Gr = 16;
-  if (Gr < 1) Gr = 1;
-  // bulk copies need 16-byte aligned rows of a multiple of 16 bytes
-  const bool tma = (n & 3) == 0 && (reinterpret_cast<uintptr_t>(R) & 15) == 0;
   unsigned mpar = 0;  // parity of the next phase of s_mbar
   if (tid == 0) {
     mbar_init(&s_mbar, 1);
@@ -245,456 +213,497 @@ __global__ void __launch_bounds__(kUrThreads, 1)
     __syncthreads();
     return ok;
   };
-  // this CTA's slice [sb, se) of atom a's c entries starting at beg
-  auto slice_of = [&](int a, int& beg, int& c, int& active, int& sb, int& se) {
-    beg = atom_ptr[a];
-    c = atom_ptr[a + 1] - beg;
-    active = ur_active(c, G, slice_target);
-    sb = int(int64_t(c) * b / active);
-    se = int(int64_t(c) * (b + 1) / active);
-  };
-  // entries, old coefficients and store-back flags of [sb, sb + cnt) into
-  // meta buffer `slot` and atom a into dst (all threads; several loads in
-  // flight per thread).  A residual row is stored back unless a is the last
-  // atom of the patch's support.
-  auto load_meta = [&](int beg, int sb, int cnt, int slot, int a, float* dst) {
-    int* ent = ent_b + slot * cap;
-    float* xo = xold_b + slot * cap;
-    int* kp = keep_b + slot * cap;
-    constexpr int kB = 4;
-    for (int t0 = tid; t0 < cnt; t0 += kUrThreads * kB) {
-      int e[kB];
-#pragma unroll
-      for (int k = 0; k < kB; ++k) {
-        const int t = t0 + k * kUrThreads;
-        e[k] = (t < cnt) ? __ldg(entries + beg + sb + t) : 0;
-      }
-      float x[kB];
-      int lt[kB];
-#pragma unroll
-      for (int k = 0; k < kB; ++k) {
-        const bool in = t0 + k * kUrThreads < cnt;
-        x[k] = in ? __ldcg(coef + e[k]) : 0.0f;
-        lt[k] = (in && last != nullptr) ? __ldg(last + e[k] / L) : -1;
-      }
-#pragma unroll
-      for (int k = 0; k < kB; ++k) {
-        const int t = t0 + k * kUrThreads;
-        if (t < cnt) {
-          ent[t] = e[k];
-          xo[t] = x[k];
-          kp[t] = (lt[k] != a) ? 1 : 0;
+
+  // every group whose CTA range holds this CTA, in the order of the table
+  for (int gi = 0; gi < batch.ngroups; ++gi) {
+    const UpdGroup& grp = batch.g[gi];
+    if (int(blockIdx.x) < grp.cta_begin || int(blockIdx.x) >= grp.cta_begin + grp.ctas) continue;
+    __syncthreads();  // the previous group's shared memory is no longer read
+    float* const R = grp.R;
+    float* const D = grp.D;
+    float* const coef = grp.coef;
+    const int* __restrict__ const atom_ptr = grp.atom_ptr;
+    const int* __restrict__ const entries = grp.entries;
+    const int* __restrict__ const last = grp.last;
+    float* const gw = grp.gw;
+    unsigned* const sync = grp.sync;
+    const int n = grp.n, K = grp.K, L = grp.L, q1_cap = grp.q1_cap, cap = grp.cap;
+    const int slice_target = grp.slice_target > 0 ? grp.slice_target : kUrDefaultSlice;
+    const int n4 = ur_n4(n), es = ur_es(n);
+    const int F = n4 / 4, es4 = es / 4;  // float4 per row of u / w, per resident column
+    float* Es = reinterpret_cast<float*>(ursm);
+    const float4* Es4 = reinterpret_cast<const float4*>(ursm);
+    int* ent_b = reinterpret_cast<int*>(ursm + size_t(cap) * es * 4);  // [2][cap]
+    float* xold_b = reinterpret_cast<float*>(ent_b + 2 * cap);           // [2][cap]
+    int* keep_b = reinterpret_cast<int*>(xold_b + 2 * cap);  // [2][cap]: residual row stored back
+    float* u = reinterpret_cast<float*>(keep_b + 2 * cap);
+    float* dold = u + n4;
+    float* dnext = dold + n4;
+    float* wred = dnext + n4;  // [kUrRows][n4]
+    float4* u4 = reinterpret_cast<float4*>(u);
+    const float4* dold4 = reinterpret_cast<const float4*>(dold);
+    float4* wred4 = reinterpret_cast<float4*>(wred);
+
+    const int G = grp.ctas, b = int(blockIdx.x) - grp.cta_begin;
+    unsigned* iter_cnt = sync;
+    unsigned* done_cnt = sync + K;
+    int Gr = kUrThreads / F;  // column groups of the w pass, partial groups of the all-reduce
+    if (Gr > 16) Gr = 16;
+    if (Gr < 1) Gr = 1;
+    // bulk copies need 16-byte aligned rows of a multiple of 16 bytes
+    const bool tma = (n & 3) == 0 && (reinterpret_cast<uintptr_t>(R) & 15) == 0;
+
+    // this CTA's slice [sb, se) of atom a's c entries starting at beg
+    auto slice_of = [&](int a, int& beg, int& c, int& active, int& sb, int& se) {
+      beg = atom_ptr[a];
+      c = atom_ptr[a + 1] - beg;
+      active = ur_active(c, G, slice_target);
+      sb = int(int64_t(c) * b / active);
+      se = int(int64_t(c) * (b + 1) / active);
+    };
+    // entries, old coefficients and store-back flags of [sb, sb + cnt) into
+    // meta buffer `slot` and atom a into dst (all threads; several loads in
+    // flight per thread).  A residual row is stored back unless a is the last
+    // atom of the patch's support.
+    auto load_meta = [&](int beg, int sb, int cnt, int slot, int a, float* dst) {
+      int* ent = ent_b + slot * cap;
+      float* xo = xold_b + slot * cap;
+      int* kp = keep_b + slot * cap;
+      constexpr int kB = 4;
+      for (int t0 = tid; t0 < cnt; t0 += kUrThreads * kB) {
+        int e[kB];
+  #pragma unroll
+        for (int k = 0; k < kB; ++k) {
+          const int t = t0 + k * kUrThreads;
+          e[k] = (t < cnt) ? __ldg(entries + beg + sb + t) : 0;
+        }
+        float x[kB];
+        int lt[kB];
+  #pragma unroll
+        for (int k = 0; k < kB; ++k) {
+          const bool in = t0 + k * kUrThreads < cnt;
+          x[k] = in ? __ldcg(coef + e[k]) : 0.0f;
+          lt[k] = (in && last != nullptr) ? __ldg(last + e[k] / L) : -1;
+        }
+  #pragma unroll
+        for (int k = 0; k < kB; ++k) {
+          const int t = t0 + k * kUrThreads;
+          if (t < cnt) {
+            ent[t] = e[k];
+            xo[t] = x[k];
+            kp[t] = (lt[k] != a) ? 1 : 0;
+          }
         }
       }
-    }
-    for (int i = tid; i < n4; i += kUrThreads) dst[i] = (i < n) ? __ldcg(D + int64_t(a) * n + i) : 0.0f;
-  };
-  // u . e_q for a resident column (one thread, 16-byte loads, 4 chains)
-  auto dot_u = [&](int q) -> float {
-    const float4* er = Es4 + size_t(q) * es4;
-    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
-#pragma unroll 6
-    for (int f = 0; f < F; ++f) {
-      const float4 e = er[f], w = u4[f];
-      a0 = fmaf(e.x, w.x, a0);
-      a1 = fmaf(e.y, w.y, a1);
-      a2 = fmaf(e.z, w.z, a2);
-      a3 = fmaf(e.w, w.w, a3);
-    }
-    return (a0 + a1) + (a2 + a3);
-  };
-
-  int jprev = -1, aprev = 0;
-  int slot = 0;        // meta buffer of the current atom
-  int meta_atom = -1;  // atom whose meta was prefetched into buffer `slot`
-  for (int j = 0; j < K; ++j) {
-    int beg, c, active, sb, se;
-    slice_of(j, beg, c, active, sb, se);
-    if (c == 0) continue;
-    const int jp = jprev, ap = aprev;
-    jprev = j;
-    aprev = active;
-    if (b >= active) continue;
-    const int c_eff = (q1_cap && c > 1024) ? 1024 : c;
-    const int m = se - sb;
-    const int mres = m < cap ? m : cap;
-    // columns [0, mc) of the slice enter the power iteration
-    int mc = c_eff - sb;
-    mc = mc < 0 ? 0 : (mc > m ? m : mc);
-    const int mcr = mc < cap ? mc : cap;  // of which resident
-    const bool streamed = mc > cap;        // some enter from the residual
-    const int* ent_s = ent_b + slot * cap;
-    const float* xold_s = xold_b + slot * cap;
-    float* v_s = xold_b + slot * cap;  // per-column scalars once the columns are built
-    const int* keep_s = keep_b + slot * cap;
-
-    // ---- entries, old coefficients and the old atom: never written by other
-    // atoms, so read before the wait (or prefetched during the previous atom)
-    if (meta_atom == j) {
-      for (int i = tid; i < n4; i += kUrThreads) dold[i] = dnext[i];
-    } else {
-      load_meta(beg, sb, mres, slot, j, dold);
-    }
-    lap(7);
-    __syncthreads();
-    if (jp >= 0 && !block_wait(done_cnt + jp, unsigned(ap))) return;
-    lap(0);
-
-    // the next non-empty atom; if this CTA works on it, its meta is fetched
-    // while this CTA waits for the first partials
-    int jn = j + 1;
-    while (jn < K && atom_ptr[jn + 1] == atom_ptr[jn]) ++jn;
-    int nbeg = 0, nc = 0, nact = 0, nsb = 0, nse = 0;
-    bool prefetch = false;
-    if (jn < K) {
-      slice_of(jn, nbeg, nc, nact, nsb, nse);
-      prefetch = b < nact;
-    }
-
-    // ---- resident columns e_q = r_q + x_q d_old ---------------------------
-    if (tma) {
-      // residual rows by bulk copies (the residual was written by other CTAs
-      // through the generic proxy: acquire above, proxy fence here), then
-      // e = r + x d in place
-      if (tid == 0) mbar_arrive_expect_tx(&s_mbar, unsigned(mres) * unsigned(n) * 4u);
-      __syncthreads();
-      asm volatile("fence.proxy.async.global;" ::: "memory");
-      for (int q = tid; q < mres; q += kUrThreads)
-        bulk_g2s(Es + size_t(q) * es, R + int64_t(ent_s[q] / L) * n, unsigned(n) * 4u, &s_mbar);
-      const bool ok = mbar_wait(&s_mbar, mpar, kBarrierTimeoutNs);
-      mpar ^= 1u;
-      if (__syncthreads_or(!ok)) {
-        if (tid == 0) atomicCAS(&flags->err, DEVERR_NONE, DEVERR_TIMEOUT);
-        return;
+      for (int i = tid; i < n4; i += kUrThreads) dst[i] = (i < n) ? __ldcg(D + int64_t(a) * n + i) : 0.0f;
+    };
+    // u . e_q for a resident column (one thread, 16-byte loads, 4 chains)
+    auto dot_u = [&](int q) -> float {
+      const float4* er = Es4 + size_t(q) * es4;
+      float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+  #pragma unroll 6
+      for (int f = 0; f < F; ++f) {
+        const float4 e = er[f], w = u4[f];
+        a0 = fmaf(e.x, w.x, a0);
+        a1 = fmaf(e.y, w.y, a1);
+        a2 = fmaf(e.z, w.z, a2);
+        a3 = fmaf(e.w, w.w, a3);
       }
-      for (int t = tid; t < mres * F; t += kUrThreads) {
-        const int q = t / F, f = t - q * F;
-        const float x = xold_s[q];
-        const float4 d = dold4[f];
-        float4* ep = reinterpret_cast<float4*>(Es) + size_t(q) * es4 + f;
-        float4 e = *ep;
-        e.x = fmaf(x, d.x, e.x);
-        e.y = fmaf(x, d.y, e.y);
-        e.z = fmaf(x, d.z, e.z);
-        e.w = fmaf(x, d.w, e.w);
-        *ep = e;
-      }
-    } else {
-      for (int t = tid; t < mres * n4; t += kUrThreads) {
-        const int q = t / n4, i = t - q * n4;
-        float e = 0.0f;
-        if (i < n) e = fmaf(xold_s[q], dold[i], __ldcg(R + int64_t(ent_s[q] / L) * n + i));
-        Es[size_t(q) * es + i] = e;
-      }
-    }
-    for (int i = tid; i < n4; i += kUrThreads) u[i] = dold[i];
-    __syncthreads();
-    lap(1);
-
-    // Two streamed columns (q0, q1 = q0 + kUrWarps, both >= cap) from the
-    // residual; a column index >= lim gives zeros.
-    auto stream_cols = [&](int q0, int lim, float (&e0)[NW], float (&e1)[NW], int& ea, int& eb) {
-      const int q1 = q0 + kUrWarps;
-      ea = (q0 < lim) ? __ldg(entries + beg + sb + q0) : -1;
-      eb = (q1 < lim) ? __ldg(entries + beg + sb + q1) : -1;
-      const float xa = (ea >= 0) ? __ldcg(coef + ea) : 0.0f;
-      const float xb = (eb >= 0) ? __ldcg(coef + eb) : 0.0f;
-      const float* ra = R + int64_t(ea >= 0 ? ea / L : 0) * n;
-      const float* rb = R + int64_t(eb >= 0 ? eb / L : 0) * n;
-#pragma unroll
-      for (int k = 0; k < NW; ++k) {
-        const int i = lane + 32 * k;
-        e0[k] = (i < n && ea >= 0) ? fmaf(xa, dold[i], __ldcg(ra + i)) : 0.0f;
-        e1[k] = (i < n && eb >= 0) ? fmaf(xb, dold[i], __ldcg(rb + i)) : 0.0f;
-      }
+      return (a0 + a1) + (a2 + a3);
     };
 
-    // ---- power iteration ---------------------------------------------------
-    int iters = 0;
-    float dprev = 0.0f;  // warp 0: the previous step's change
-    for (int it = 0; it < kUrMaxIters; ++it) {
-      // v_q = u . e_q, one thread per resident column
-      for (int q = tid; q < mcr; q += kUrThreads) v_s[q] = dot_u(q);
-      if (streamed) {  // columns beyond the capacity: a warp per two columns
-        float ur[NW], wacc[NW];
-#pragma unroll
+    int jprev = -1, aprev = 0;
+    int slot = 0;        // meta buffer of the current atom
+    int meta_atom = -1;  // atom whose meta was prefetched into buffer `slot`
+    for (int j = 0; j < K; ++j) {
+      int beg, c, active, sb, se;
+      slice_of(j, beg, c, active, sb, se);
+      if (c == 0) continue;
+      const int jp = jprev, ap = aprev;
+      jprev = j;
+      aprev = active;
+      if (b >= active) continue;
+      const int c_eff = (q1_cap && c > 1024) ? 1024 : c;
+      const int m = se - sb;
+      const int mres = m < cap ? m : cap;
+      // columns [0, mc) of the slice enter the power iteration
+      int mc = c_eff - sb;
+      mc = mc < 0 ? 0 : (mc > m ? m : mc);
+      const int mcr = mc < cap ? mc : cap;  // of which resident
+      const bool streamed = mc > cap;        // some enter from the residual
+      const int* ent_s = ent_b + slot * cap;
+      const float* xold_s = xold_b + slot * cap;
+      float* v_s = xold_b + slot * cap;  // per-column scalars once the columns are built
+      const int* keep_s = keep_b + slot * cap;
+
+      // ---- entries, old coefficients and the old atom: never written by other
+      // atoms, so read before the wait (or prefetched during the previous atom)
+      if (meta_atom == j) {
+        for (int i = tid; i < n4; i += kUrThreads) dold[i] = dnext[i];
+      } else {
+        load_meta(beg, sb, mres, slot, j, dold);
+      }
+      lap(7);
+      __syncthreads();
+      if (jp >= 0 && !block_wait(done_cnt + jp, unsigned(ap))) return;
+      lap(0);
+
+      // the next non-empty atom; if this CTA works on it, its meta is fetched
+      // while this CTA waits for the first partials
+      int jn = j + 1;
+      while (jn < K && atom_ptr[jn + 1] == atom_ptr[jn]) ++jn;
+      int nbeg = 0, nc = 0, nact = 0, nsb = 0, nse = 0;
+      bool prefetch = false;
+      if (jn < K) {
+        slice_of(jn, nbeg, nc, nact, nsb, nse);
+        prefetch = b < nact;
+      }
+
+      // ---- resident columns e_q = r_q + x_q d_old ---------------------------
+      if (tma) {
+        // residual rows by bulk copies (the residual was written by other CTAs
+        // through the generic proxy: acquire above, proxy fence here), then
+        // e = r + x d in place
+        if (tid == 0) mbar_arrive_expect_tx(&s_mbar, unsigned(mres) * unsigned(n) * 4u);
+        __syncthreads();
+        asm volatile("fence.proxy.async.global;" ::: "memory");
+        for (int q = tid; q < mres; q += kUrThreads)
+          bulk_g2s(Es + size_t(q) * es, R + int64_t(ent_s[q] / L) * n, unsigned(n) * 4u, &s_mbar);
+        const bool ok = mbar_wait(&s_mbar, mpar, kBarrierTimeoutNs);
+        mpar ^= 1u;
+        if (__syncthreads_or(!ok)) {
+          if (tid == 0) atomicCAS(&flags->err, DEVERR_NONE, DEVERR_TIMEOUT);
+          return;
+        }
+        for (int t = tid; t < mres * F; t += kUrThreads) {
+          const int q = t / F, f = t - q * F;
+          const float x = xold_s[q];
+          const float4 d = dold4[f];
+          float4* ep = reinterpret_cast<float4*>(Es) + size_t(q) * es4 + f;
+          float4 e = *ep;
+          e.x = fmaf(x, d.x, e.x);
+          e.y = fmaf(x, d.y, e.y);
+          e.z = fmaf(x, d.z, e.z);
+          e.w = fmaf(x, d.w, e.w);
+          *ep = e;
+        }
+      } else {
+        for (int t = tid; t < mres * n4; t += kUrThreads) {
+          const int q = t / n4, i = t - q * n4;
+          float e = 0.0f;
+          if (i < n) e = fmaf(xold_s[q], dold[i], __ldcg(R + int64_t(ent_s[q] / L) * n + i));
+          Es[size_t(q) * es + i] = e;
+        }
+      }
+      for (int i = tid; i < n4; i += kUrThreads) u[i] = dold[i];
+      __syncthreads();
+      lap(1);
+
+      // Two streamed columns (q0, q1 = q0 + kUrWarps, both >= cap) from the
+      // residual; a column index >= lim gives zeros.
+      auto stream_cols = [&](int q0, int lim, float (&e0)[NW], float (&e1)[NW], int& ea, int& eb) {
+        const int q1 = q0 + kUrWarps;
+        ea = (q0 < lim) ? __ldg(entries + beg + sb + q0) : -1;
+        eb = (q1 < lim) ? __ldg(entries + beg + sb + q1) : -1;
+        const float xa = (ea >= 0) ? __ldcg(coef + ea) : 0.0f;
+        const float xb = (eb >= 0) ? __ldcg(coef + eb) : 0.0f;
+        const float* ra = R + int64_t(ea >= 0 ? ea / L : 0) * n;
+        const float* rb = R + int64_t(eb >= 0 ? eb / L : 0) * n;
+  #pragma unroll
         for (int k = 0; k < NW; ++k) {
           const int i = lane + 32 * k;
-          ur[k] = (i < n) ? u[i] : 0.0f;
-          wacc[k] = 0.0f;
+          e0[k] = (i < n && ea >= 0) ? fmaf(xa, dold[i], __ldcg(ra + i)) : 0.0f;
+          e1[k] = (i < n && eb >= 0) ? fmaf(xb, dold[i], __ldcg(rb + i)) : 0.0f;
         }
-        for (int q = cap + warp; q < mc; q += 2 * kUrWarps) {
-          float e0[NW], e1[NW];
-          int ea, eb;
-          stream_cols(q, mc, e0, e1, ea, eb);
-          float d0 = 0.0f, d1 = 0.0f;
-#pragma unroll
+      };
+
+      // ---- power iteration ---------------------------------------------------
+      int iters = 0;
+      float dprev = 0.0f;  // warp 0: the previous step's change
+      for (int it = 0; it < kUrMaxIters; ++it) {
+        // v_q = u . e_q, one thread per resident column
+        for (int q = tid; q < mcr; q += kUrThreads) v_s[q] = dot_u(q);
+        if (streamed) {  // columns beyond the capacity: a warp per two columns
+          float ur[NW], wacc[NW];
+  #pragma unroll
           for (int k = 0; k < NW; ++k) {
-            d0 = fmaf(ur[k], e0[k], d0);
-            d1 = fmaf(ur[k], e1[k], d1);
+            const int i = lane + 32 * k;
+            ur[k] = (i < n) ? u[i] : 0.0f;
+            wacc[k] = 0.0f;
           }
-#pragma unroll
-          for (int o = 16; o > 0; o >>= 1) {
-            d0 += __shfl_xor_sync(0xffffffffu, d0, o);
-            d1 += __shfl_xor_sync(0xffffffffu, d1, o);
+          for (int q = cap + warp; q < mc; q += 2 * kUrWarps) {
+            float e0[NW], e1[NW];
+            int ea, eb;
+            stream_cols(q, mc, e0, e1, ea, eb);
+            float d0 = 0.0f, d1 = 0.0f;
+  #pragma unroll
+            for (int k = 0; k < NW; ++k) {
+              d0 = fmaf(ur[k], e0[k], d0);
+              d1 = fmaf(ur[k], e1[k], d1);
+            }
+  #pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+              d0 += __shfl_xor_sync(0xffffffffu, d0, o);
+              d1 += __shfl_xor_sync(0xffffffffu, d1, o);
+            }
+  #pragma unroll
+            for (int k = 0; k < NW; ++k) wacc[k] = fmaf(d1, e1[k], fmaf(d0, e0[k], wacc[k]));
           }
-#pragma unroll
-          for (int k = 0; k < NW; ++k) wacc[k] = fmaf(d1, e1[k], fmaf(d0, e0[k], wacc[k]));
-        }
-#pragma unroll
-        for (int k = 0; k < NW; ++k) {
-          const int i = lane + 32 * k;
-          if (i < n4) wred[(16 + warp) * n4 + i] = wacc[k];
-        }
-      }
-      __syncthreads();
-      // w = sum_q v_q e_q: column group g (q = g mod Gr) of float4 column f
-      {
-        const int f = tid % F, g = tid / F;
-        if (g < Gr) {
-          float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll 4
-          for (int q = g; q < mcr; q += Gr) {
-            const float v = v_s[q];
-            const float4 e = Es4[size_t(q) * es4 + f];
-            acc.x = fmaf(v, e.x, acc.x);
-            acc.y = fmaf(v, e.y, acc.y);
-            acc.z = fmaf(v, e.z, acc.z);
-            acc.w = fmaf(v, e.w, acc.w);
+  #pragma unroll
+          for (int k = 0; k < NW; ++k) {
+            const int i = lane + 32 * k;
+            if (i < n4) wred[(16 + warp) * n4 + i] = wacc[k];
           }
-          wred4[g * F + f] = acc;
         }
-      }
-      __syncthreads();
-      float4* gwp = reinterpret_cast<float4*>(gw + (size_t(it & 1) * G + b) * n4);
-      for (int f = tid; f < F; f += kUrThreads) {
-        float4 acc = wred4[f];
-#pragma unroll 4
-        for (int g = 1; g < Gr; ++g) {
-          const float4 v = wred4[g * F + f];
-          acc.x += v.x;
-          acc.y += v.y;
-          acc.z += v.z;
-          acc.w += v.w;
+        __syncthreads();
+        // w = sum_q v_q e_q: column group g (q = g mod Gr) of float4 column f
+        {
+          const int f = tid % F, g = tid / F;
+          if (g < Gr) {
+            float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+  #pragma unroll 4
+            for (int q = g; q < mcr; q += Gr) {
+              const float v = v_s[q];
+              const float4 e = Es4[size_t(q) * es4 + f];
+              acc.x = fmaf(v, e.x, acc.x);
+              acc.y = fmaf(v, e.y, acc.y);
+              acc.z = fmaf(v, e.z, acc.z);
+              acc.w = fmaf(v, e.w, acc.w);
+            }
+            wred4[g * F + f] = acc;
+          }
         }
-        if (streamed)
-#pragma unroll
-          for (int w = 0; w < kUrWarps; ++w) {
-            const float4 v = wred4[(16 + w) * F + f];
+        __syncthreads();
+        float4* gwp = reinterpret_cast<float4*>(gw + (size_t(it & 1) * G + b) * n4);
+        for (int f = tid; f < F; f += kUrThreads) {
+          float4 acc = wred4[f];
+  #pragma unroll 4
+          for (int g = 1; g < Gr; ++g) {
+            const float4 v = wred4[g * F + f];
             acc.x += v.x;
             acc.y += v.y;
             acc.z += v.z;
             acc.w += v.w;
           }
-        __stcg(gwp + f, acc);
-      }
-      __syncthreads();
-      lap(2);
-      if (tid == 0) red_release_add(iter_cnt + j, 1u);
-      if (it == 0 && prefetch)  // overlaps the wait below
-        load_meta(nbeg, nsb, min(nse - nsb, cap), slot ^ 1, jn, dnext);
-      if (!block_wait(iter_cnt + j, unsigned(it + 1) * unsigned(active))) return;
-      lap(3);
-      // all-reduce: group g sums partials g, g + Gr, ... of float4 column f in
-      // ascending order (loads batched)
-      {
-        const int f = tid % F, g = tid / F;
-        if (g < Gr) {
-          float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-          const float4* base = reinterpret_cast<const float4*>(gw + size_t(it & 1) * G * n4) + f;
-          constexpr int kB = 12;  // one round of loads for up to 12 Gr partials per thread
-          for (int bb0 = g; bb0 < active; bb0 += Gr * kB) {
-            float4 v[kB];
-#pragma unroll
-            for (int k = 0; k < kB; ++k) {
-              const int bb = bb0 + k * Gr;
-              v[k] = (bb < active) ? __ldcg(base + size_t(bb) * F) : make_float4(0.f, 0.f, 0.f, 0.f);
-            }
-#pragma unroll
-            for (int k = 0; k < kB; ++k) {
-              acc.x += v[k].x;
-              acc.y += v[k].y;
-              acc.z += v[k].z;
-              acc.w += v[k].w;
-            }
-          }
-          wred4[g * F + f] = acc;
-        }
-      }
-      __syncthreads();
-      iters = it + 1;
-      // warp 0 finishes the step: w, its norm, the new u, the change, the
-      // stop decision and, when stopping, the sign (u . d_old >= 0)
-      if (warp == 0) {
-        constexpr int kF = 4;  // float4 per lane (F <= 128)
-        float4 wv[kF];
-        float s2 = 0.0f;
-#pragma unroll
-        for (int k = 0; k < kF; ++k) {
-          const int f = lane + 32 * k;
-          float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-          if (f < F)
-#pragma unroll 4
-            for (int g = 0; g < Gr; ++g) {
-              const float4 v = wred4[g * F + f];
+          if (streamed)
+  #pragma unroll
+            for (int w = 0; w < kUrWarps; ++w) {
+              const float4 v = wred4[(16 + w) * F + f];
               acc.x += v.x;
               acc.y += v.y;
               acc.z += v.z;
               acc.w += v.w;
             }
-          wv[k] = acc;
-          s2 = fmaf(acc.x, acc.x, fmaf(acc.y, acc.y, fmaf(acc.z, acc.z, fmaf(acc.w, acc.w, s2))));
+          __stcg(gwp + f, acc);
         }
-        const float nrm2 = warp_sum(s2);
-        bool stop;
-        if (!(nrm2 > 0.0f)) {
-          stop = true;  // E == 0: keep the old atom direction
-        } else {
-          const float inv = 1.0f / sqrtf(nrm2);
-          float dm = 0.0f;
-#pragma unroll
+        __syncthreads();
+        lap(2);
+        if (tid == 0) red_release_add(iter_cnt + j, 1u);
+        if (it == 0 && prefetch)  // overlaps the wait below
+          load_meta(nbeg, nsb, min(nse - nsb, cap), slot ^ 1, jn, dnext);
+        if (!block_wait(iter_cnt + j, unsigned(it + 1) * unsigned(active))) return;
+        lap(3);
+        // all-reduce: group g sums partials g, g + Gr, ... of float4 column f in
+        // ascending order (loads batched)
+        {
+          const int f = tid % F, g = tid / F;
+          if (g < Gr) {
+            float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+            const float4* base = reinterpret_cast<const float4*>(gw + size_t(it & 1) * G * n4) + f;
+            constexpr int kB = 12;  // one round of loads for up to 12 Gr partials per thread
+            for (int bb0 = g; bb0 < active; bb0 += Gr * kB) {
+              float4 v[kB];
+  #pragma unroll
+              for (int k = 0; k < kB; ++k) {
+                const int bb = bb0 + k * Gr;
+                v[k] = (bb < active) ? __ldcg(base + size_t(bb) * F) : make_float4(0.f, 0.f, 0.f, 0.f);
+              }
+  #pragma unroll
+              for (int k = 0; k < kB; ++k) {
+                acc.x += v[k].x;
+                acc.y += v[k].y;
+                acc.z += v[k].z;
+                acc.w += v[k].w;
+              }
+            }
+            wred4[g * F + f] = acc;
+          }
+        }
+        __syncthreads();
+        iters = it + 1;
+        // warp 0 finishes the step: w, its norm, the new u, the change, the
+        // stop decision and, when stopping, the sign (u . d_old >= 0)
+        if (warp == 0) {
+          constexpr int kF = 4;  // float4 per lane (F <= 128)
+          float4 wv[kF];
+          float s2 = 0.0f;
+  #pragma unroll
           for (int k = 0; k < kF; ++k) {
             const int f = lane + 32 * k;
-            if (f < F) {
-              const float4 o = u4[f];
-              float4 un;
-              un.x = wv[k].x * inv;
-              un.y = wv[k].y * inv;
-              un.z = wv[k].z * inv;
-              un.w = wv[k].w * inv;
-              dm = fmaxf(dm, fmaxf(fmaxf(fabsf(un.x - o.x), fabsf(un.y - o.y)),
-                                   fmaxf(fabsf(un.z - o.z), fabsf(un.w - o.w))));
-              u4[f] = un;
-            }
+            float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (f < F)
+  #pragma unroll 4
+              for (int g = 0; g < Gr; ++g) {
+                const float4 v = wred4[g * F + f];
+                acc.x += v.x;
+                acc.y += v.y;
+                acc.z += v.z;
+                acc.w += v.w;
+              }
+            wv[k] = acc;
+            s2 = fmaf(acc.x, acc.x, fmaf(acc.y, acc.y, fmaf(acc.z, acc.z, fmaf(acc.w, acc.w, s2))));
           }
-          dm = warp_max(dm);
-          // stop when the change is below the tolerance, or when the observed
-          // contraction rho = dm / dprev puts the remaining distance to the
-          // limit, about dm rho / (1 - rho), below it
-          const float rho = (it > 0 && dprev > 0.0f) ? dm / dprev : 1.0f;
-          stop = dm < kUrTol || (rho < 0.5f && dm < 1e-3f && dm * rho < kUrTol * (1.0f - rho));
-          dprev = dm;
-        }
-        if (stop) {
-          float sd = 0.0f;
-#pragma unroll
-          for (int k = 0; k < kF; ++k) {
-            const int f = lane + 32 * k;
-            if (f < F) {
-              const float4 a = u4[f], d = dold4[f];
-              sd = fmaf(a.x, d.x, fmaf(a.y, d.y, fmaf(a.z, d.z, fmaf(a.w, d.w, sd))));
-            }
-          }
-          sd = warp_sum(sd);
-          if (sd < 0.0f)
-#pragma unroll
+          const float nrm2 = warp_sum(s2);
+          bool stop;
+          if (!(nrm2 > 0.0f)) {
+            stop = true;  // E == 0: keep the old atom direction
+          } else {
+            const float inv = 1.0f / sqrtf(nrm2);
+            float dm = 0.0f;
+  #pragma unroll
             for (int k = 0; k < kF; ++k) {
               const int f = lane + 32 * k;
               if (f < F) {
-                float4 a = u4[f];
-                a.x = -a.x;
-                a.y = -a.y;
-                a.z = -a.z;
-                a.w = -a.w;
-                u4[f] = a;
+                const float4 o = u4[f];
+                float4 un;
+                un.x = wv[k].x * inv;
+                un.y = wv[k].y * inv;
+                un.z = wv[k].z * inv;
+                un.w = wv[k].w * inv;
+                dm = fmaxf(dm, fmaxf(fmaxf(fabsf(un.x - o.x), fabsf(un.y - o.y)),
+                                     fmaxf(fabsf(un.z - o.z), fabsf(un.w - o.w))));
+                u4[f] = un;
               }
             }
-        }
-        if (lane == 0) s_stop = stop ? 1 : 0;
-      }
-      __syncthreads();
-      lap(4);
-      if (s_stop) break;
-    }
-    if (b == 0) {
-      for (int i = tid; i < n; i += kUrThreads) __stcg(D + int64_t(j) * n + i, u[i]);
-      if (tid == 0) {
-        atomicAdd(&stats->power_iters, (unsigned long long)iters);
-        atomicAdd(&stats->atoms_updated, 1ull);
-      }
-    }
-
-    // ---- coefficients x = u . e (0 beyond the cap) and residual e - x u ----
-    for (int q = tid; q < mres; q += kUrThreads) {
-      const float x = (q < mc) ? dot_u(q) : 0.0f;
-      v_s[q] = x;
-      __stcg(coef + ent_s[q], x);
-    }
-    if (m > cap) {  // streamed columns: a warp per two columns
-      float ur[NW];
-#pragma unroll
-      for (int k = 0; k < NW; ++k) {
-        const int i = lane + 32 * k;
-        ur[k] = (i < n) ? u[i] : 0.0f;
-      }
-      for (int q = cap + warp; q < m; q += 2 * kUrWarps) {
-        float e0[NW], e1[NW];
-        int ea, eb;
-        stream_cols(q, m, e0, e1, ea, eb);
-        float x0 = 0.0f, x1 = 0.0f;
-#pragma unroll
-        for (int k = 0; k < NW; ++k) {
-          x0 = fmaf(ur[k], e0[k], x0);
-          x1 = fmaf(ur[k], e1[k], x1);
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          x0 += __shfl_xor_sync(0xffffffffu, x0, o);
-          x1 += __shfl_xor_sync(0xffffffffu, x1, o);
-        }
-        if (q >= mc) x0 = 0.0f;
-        if (q + kUrWarps >= mc) x1 = 0.0f;
-        float* ra = R + int64_t(ea / L) * n;
-        if (last == nullptr || __ldg(last + ea / L) != j) {
-#pragma unroll
-          for (int k = 0; k < NW; ++k) {
-            const int i = lane + 32 * k;
-            if (i < n) __stcg(ra + i, fmaf(-x0, ur[k], e0[k]));
+            dm = warp_max(dm);
+            // stop when the change is below the tolerance, or when the observed
+            // contraction rho = dm / dprev puts the remaining distance to the
+            // limit, about dm rho / (1 - rho), below it
+            const float rho = (it > 0 && dprev > 0.0f) ? dm / dprev : 1.0f;
+            stop = dm < kUrTol || (rho < 0.5f && dm < 1e-3f && dm * rho < kUrTol * (1.0f - rho));
+            dprev = dm;
           }
+          if (stop) {
+            float sd = 0.0f;
+  #pragma unroll
+            for (int k = 0; k < kF; ++k) {
+              const int f = lane + 32 * k;
+              if (f < F) {
+                const float4 a = u4[f], d = dold4[f];
+                sd = fmaf(a.x, d.x, fmaf(a.y, d.y, fmaf(a.z, d.z, fmaf(a.w, d.w, sd))));
+              }
+            }
+            sd = warp_sum(sd);
+            if (sd < 0.0f)
+  #pragma unroll
+              for (int k = 0; k < kF; ++k) {
+                const int f = lane + 32 * k;
+                if (f < F) {
+                  float4 a = u4[f];
+                  a.x = -a.x;
+                  a.y = -a.y;
+                  a.z = -a.z;
+                  a.w = -a.w;
+                  u4[f] = a;
+                }
+              }
+          }
+          if (lane == 0) s_stop = stop ? 1 : 0;
         }
-        if (lane == 0) __stcg(coef + ea, x0);
-        if (eb >= 0) {
-          float* rb = R + int64_t(eb / L) * n;
-          if (last == nullptr || __ldg(last + eb / L) != j) {
-#pragma unroll
+        __syncthreads();
+        lap(4);
+        if (s_stop) break;
+      }
+      if (b == 0) {
+        for (int i = tid; i < n; i += kUrThreads) __stcg(D + int64_t(j) * n + i, u[i]);
+        if (tid == 0) {
+          atomicAdd(&stats->power_iters, (unsigned long long)iters);
+          atomicAdd(&stats->atoms_updated, 1ull);
+        }
+      }
+
+      // ---- coefficients x = u . e (0 beyond the cap) and residual e - x u ----
+      for (int q = tid; q < mres; q += kUrThreads) {
+        const float x = (q < mc) ? dot_u(q) : 0.0f;
+        v_s[q] = x;
+        __stcg(coef + ent_s[q], x);
+      }
+      if (m > cap) {  // streamed columns: a warp per two columns
+        float ur[NW];
+  #pragma unroll
+        for (int k = 0; k < NW; ++k) {
+          const int i = lane + 32 * k;
+          ur[k] = (i < n) ? u[i] : 0.0f;
+        }
+        for (int q = cap + warp; q < m; q += 2 * kUrWarps) {
+          float e0[NW], e1[NW];
+          int ea, eb;
+          stream_cols(q, m, e0, e1, ea, eb);
+          float x0 = 0.0f, x1 = 0.0f;
+  #pragma unroll
+          for (int k = 0; k < NW; ++k) {
+            x0 = fmaf(ur[k], e0[k], x0);
+            x1 = fmaf(ur[k], e1[k], x1);
+          }
+  #pragma unroll
+          for (int o = 16; o > 0; o >>= 1) {
+            x0 += __shfl_xor_sync(0xffffffffu, x0, o);
+            x1 += __shfl_xor_sync(0xffffffffu, x1, o);
+          }
+          if (q >= mc) x0 = 0.0f;
+          if (q + kUrWarps >= mc) x1 = 0.0f;
+          float* ra = R + int64_t(ea / L) * n;
+          if (last == nullptr || __ldg(last + ea / L) != j) {
+  #pragma unroll
             for (int k = 0; k < NW; ++k) {
               const int i = lane + 32 * k;
-              if (i < n) __stcg(rb + i, fmaf(-x1, ur[k], e1[k]));
+              if (i < n) __stcg(ra + i, fmaf(-x0, ur[k], e0[k]));
             }
           }
-          if (lane == 0) __stcg(coef + eb, x1);
+          if (lane == 0) __stcg(coef + ea, x0);
+          if (eb >= 0) {
+            float* rb = R + int64_t(eb / L) * n;
+            if (last == nullptr || __ldg(last + eb / L) != j) {
+  #pragma unroll
+              for (int k = 0; k < NW; ++k) {
+                const int i = lane + 32 * k;
+                if (i < n) __stcg(rb + i, fmaf(-x1, ur[k], e1[k]));
+              }
+            }
+            if (lane == 0) __stcg(coef + eb, x1);
+          }
         }
       }
-    }
-    __syncthreads();
-    if (tma) {  // rows of 16-byte aligned float4
-      for (int t = tid; t < mres * F; t += kUrThreads) {
-        const int q = t / F, f = t - q * F;
-        if (!keep_s[q]) continue;
-        const float x = v_s[q];
-        const float4 e = Es4[size_t(q) * es4 + f], w = u4[f];
-        float4 r;
-        r.x = fmaf(-x, w.x, e.x);
-        r.y = fmaf(-x, w.y, e.y);
-        r.z = fmaf(-x, w.z, e.z);
-        r.w = fmaf(-x, w.w, e.w);
-        __stcg(reinterpret_cast<float4*>(R + int64_t(ent_s[q] / L) * n) + f, r);
+      __syncthreads();
+      if (tma) {  // rows of 16-byte aligned float4
+        for (int t = tid; t < mres * F; t += kUrThreads) {
+          const int q = t / F, f = t - q * F;
+          if (!keep_s[q]) continue;
+          const float x = v_s[q];
+          const float4 e = Es4[size_t(q) * es4 + f], w = u4[f];
+          float4 r;
+          r.x = fmaf(-x, w.x, e.x);
+          r.y = fmaf(-x, w.y, e.y);
+          r.z = fmaf(-x, w.z, e.z);
+          r.w = fmaf(-x, w.w, e.w);
+          __stcg(reinterpret_cast<float4*>(R + int64_t(ent_s[q] / L) * n) + f, r);
+        }
+      } else {
+        for (int t = tid; t < mres * n; t += kUrThreads) {
+          const int q = t / n, i = t - q * n;
+          if (keep_s[q]) __stcg(R + int64_t(ent_s[q] / L) * n + i, fmaf(-v_s[q], u[i], Es[size_t(q) * es + i]));
+        }
       }
-    } else {
-      for (int t = tid; t < mres * n; t += kUrThreads) {
-        const int q = t / n, i = t - q * n;
-        if (keep_s[q]) __stcg(R + int64_t(ent_s[q] / L) * n + i, fmaf(-v_s[q], u[i], Es[size_t(q) * es + i]));
+      fence_proxy_async_smem();  // generic accesses of Es before the next bulk copies into it
+      __syncthreads();
+      if (tid == 0) red_release_add(done_cnt + j, 1u);
+      lap(5);
+      if (prefetch) {
+        slot ^= 1;
+        meta_atom = jn;
+      } else {
+        meta_atom = -1;
       }
-    }
-    fence_proxy_async_smem();  // generic accesses of Es before the next bulk copies into it
-    __syncthreads();
-    if (tid == 0) red_release_add(done_cnt + j, 1u);
-    lap(5);
-    if (prefetch) {
-      slot ^= 1;
-      meta_atom = jn;
-    } else {
-      meta_atom = -1;
     }
   }
   if (timer)
@@ -763,12 +772,9 @@ cudaError_t launch_update_batch(const UpdBatch& batch, GridBarrier* flags, DevSt
   for (int i = 0; i < batch.ngroups; ++i) {
     const UpdGroup& g = batch.g[i];
     if (g.ctas < 1 || g.cta_begin < 0 || g.cta_begin + g.ctas > grid) return cudaErrorInvalidValue;
-    if (i > 0 && g.cta_begin != batch.g[i - 1].cta_begin + batch.g[i - 1].ctas) return cudaErrorInvalidValue;
     if (g.cap < 16 || g.cap > update_res_capacity(g.n)) return cudaErrorInvalidValue;
     nmax = g.n > nmax ? g.n : nmax;
   }
-  if (batch.g[0].cta_begin != 0 || batch.g[batch.ngroups - 1].cta_begin + batch.g[batch.ngroups - 1].ctas != grid)
-    return cudaErrorInvalidValue;
   void* fn = pick_update_res(nmax);
   if (!fn) return cudaErrorInvalidValue;
   size_t smem = 0;

@@ -4,13 +4,17 @@
 // kSvd (cuda_svd_denoiser.cu:368-408).  Here every image keeps its own
 // context (dictionary, codes, workspace) and stream; per K-SVD iteration the
 // images' OMP, atom lists and residuals run concurrently on a pool of
-// streams, then ONE persistent cooperative launch sweeps every image's atoms
-// at once, the SMs split between the images in proportion to their sweep
-// work (one CTA group per image, groups never wait on one another).  From
-// the second iteration on, the whole batch iteration (fork, per-image work,
-// the shared sweep, join) is captured once as a CUDA graph and replayed.
-// With tuning on, the split of the SMs is chosen by timing one sweep for
-// each candidate weighting on the first iteration's codes.
+// streams, then ONE persistent cooperative launch sweeps every image's atoms.
+// The launch's CTAs form lanes: a lane runs its images' sweeps one after the
+// other, lanes run side by side.  The plan comes from a model of one image's
+// sweep time on w CTAs (a latency floor per atom plus the local work spread
+// over the CTAs, dearer when the columns overflow shared memory): small
+// images, bound by the floor, share narrow lanes, while the images whose
+// columns need many CTAs take a wide lane in turn.  From the second
+// iteration on, the whole batch iteration (fork, per-image work, the shared
+// sweep, join) is captured once as a CUDA graph and replayed.  With tuning
+// on, the three best modelled plans are timed on the first iteration's
+// codes and the fastest is kept.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -34,30 +38,159 @@ struct Job {
   int32_t* d_idx = nullptr;
 };
 
-// CTAs per job: weights w_i^alpha with w_i the bytes one sweep moves
-// (N L (4n + 8)), at least one CTA each, largest remainders, summing to G.
-std::vector<int> split_ctas(const std::vector<double>& w, double alpha, int G) {
-  const int m = int(w.size());
-  std::vector<double> v(m);
-  double tot = 0.0;
-  for (int i = 0; i < m; ++i) tot += (v[i] = std::pow(w[i], alpha));
-  std::vector<int> c(m, 1);
-  int left = G - m;
-  std::vector<std::pair<double, int>> rem;
-  int used = 0;
-  for (int i = 0; i < m; ++i) {
-    const double share = double(left) * v[i] / tot;
-    const int f = int(share);
-    c[i] += f;
-    used += f;
-    rem.emplace_back(share - f, i);
+// One image as the sweep planner sees it: patches, features, atoms, atoms per
+// patch and the update kernel's resident columns per CTA.
+struct LaneShape {
+  double N;
+  int n, K, L, cap;
+};
+
+// CTA lanes of the shared sweep: lane l owns CTAs [begin, begin + width) and
+// runs its images one after the other; ms: its modelled time.
+struct LanePlan {
+  std::vector<int> begin, width;
+  std::vector<std::vector<int>> imgs;
+  std::vector<double> ms;
+  double total_ms = 0.0;
+};
+
+// Sweep time of one image on w CTAs (ms), a model measured on B200 with the
+// update kernel (one image at a time on every SM, 64 images of 8 x 8 to
+// 22 x 22 patches): per atom a latency floor of 11 + 0.025 n us (the
+// all-reduces and the hand-over between atoms), plus the local passes over
+// the atom's columns, 8.6e-4 us per column and feature spread over the w
+// CTAs, five times dearer for columns beyond a CTA's shared-memory capacity
+// (streamed from memory on every power step).
+double sweep_model_ms(const LaneShape& s, int w) {
+  const double E = s.N * s.L / double(s.K);  // entries per atom
+  const double floor_us = 11.0 + 0.025 * s.n;
+  const double work_us = 8.6e-4 * s.n * s.N * s.L / double(w);
+  const double streamed = std::max(0.0, 1.0 - double(s.cap) * w / E);
+  return (s.K * floor_us + work_us * (1.0 + 4.0 * streamed)) * 1e-3;
+}
+
+// Longest-processing-time-first assignment of `imgs` to lanes of the given
+// widths starting at CTA `begin0`; appended to `plan`, returns the longest
+// lane's modelled time.
+double lpt_lanes(const std::vector<LaneShape>& sh, std::vector<int> imgs, const std::vector<int>& widths, int begin0,
+                 LanePlan& plan) {
+  const int wmax = *std::max_element(widths.begin(), widths.end());
+  std::sort(imgs.begin(), imgs.end(), [&](int x, int y) {
+    const double tx = sweep_model_ms(sh[size_t(x)], wmax), ty = sweep_model_ms(sh[size_t(y)], wmax);
+    return tx > ty || (tx == ty && x < y);
+  });
+  const size_t l0 = plan.width.size();
+  int b = begin0;
+  for (int w : widths) {
+    plan.begin.push_back(b);
+    plan.width.push_back(w);
+    plan.imgs.emplace_back();
+    plan.ms.push_back(0.0);
+    b += w;
   }
-  std::sort(rem.begin(), rem.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
-  for (int k = 0; k < left - used; ++k) c[rem[size_t(k) % rem.size()].second] += 1;
-  return c;
+  for (int i : imgs) {
+    size_t best = l0;
+    double fin = 1e300;
+    for (size_t l = l0; l < plan.width.size(); ++l) {
+      const double f = plan.ms[l] + sweep_model_ms(sh[size_t(i)], plan.width[l]);
+      if (f < fin) {
+        fin = f;
+        best = l;
+      }
+    }
+    plan.ms[best] = fin;
+    plan.imgs[best].push_back(i);
+  }
+  double mx = 0.0;
+  for (size_t l = l0; l < plan.width.size(); ++l) mx = std::max(mx, plan.ms[l]);
+  return mx;
+}
+
+std::vector<int> even_widths(int total, int k) {
+  std::vector<int> w(size_t(k), total / k);
+  for (int r = 0; r < total % k; ++r) w[size_t(r)] += 1;
+  return w;
+}
+
+// Candidate lane plans for the shared sweep, best modelled first:
+//  * k equal lanes, images assigned longest first;
+//  * one wide lane of W CTAs running the nb images that take longest there,
+//    one after the other, and k equal lanes on the remaining CTAs for the rest.
+std::vector<LanePlan> lane_plans(const std::vector<LaneShape>& sh, int G) {
+  const int m = int(sh.size());
+  std::vector<LanePlan> out;
+  std::vector<int> all(static_cast<size_t>(m));
+  for (int i = 0; i < m; ++i) all[size_t(i)] = i;
+  for (int k : {1, 2, 3, 4, 6, 8, 12, 16, 24, 32}) {
+    if (k > m || k > G) continue;
+    LanePlan p;
+    p.total_ms = lpt_lanes(sh, all, even_widths(G, k), 0, p);
+    out.push_back(std::move(p));
+  }
+  for (int W : {G / 2, (2 * G) / 3, (3 * G) / 4, (5 * G) / 6}) {
+    if (W < 1 || W >= G) continue;
+    std::vector<int> by_t = all;
+    std::sort(by_t.begin(), by_t.end(), [&](int x, int y) {
+      const double tx = sweep_model_ms(sh[size_t(x)], W), ty = sweep_model_ms(sh[size_t(y)], W);
+      return tx > ty || (tx == ty && x < y);
+    });
+    for (int nb = 1; nb < m; ++nb) {
+      for (int k : {1, 2, 4, 8, 16}) {
+        if (k > G - W || k > m - nb) continue;
+        LanePlan p;
+        const std::vector<int> big(by_t.begin(), by_t.begin() + nb), rest(by_t.begin() + nb, by_t.end());
+        const double tb = lpt_lanes(sh, big, {W}, 0, p);
+        const double tr = lpt_lanes(sh, rest, even_widths(G - W, k), W, p);
+        p.total_ms = std::max(tb, tr);
+        out.push_back(std::move(p));
+      }
+    }
+  }
+  std::stable_sort(out.begin(), out.end(), [](const LanePlan& x, const LanePlan& y) { return x.total_ms < y.total_ms; });
+  return out;
+}
+
+// A plan as per-image CTA ranges and the group order of the sweep (lane by
+// lane, images of a lane in sequence).
+void plan_ranges(const LanePlan& p, int m, std::vector<int>& begin, std::vector<int>& ctas, std::vector<int>& order) {
+  begin.assign(size_t(m), 0);
+  ctas.assign(size_t(m), 0);
+  order.clear();
+  for (size_t l = 0; l < p.width.size(); ++l)
+    for (int i : p.imgs[l]) {
+      begin[size_t(i)] = p.begin[l];
+      ctas[size_t(i)] = p.width[l];
+      order.push_back(i);
+    }
 }
 
 }  // namespace
+
+extern "C" ksvd_status ksvd_many_plan(const ksvd_image_job* jobs, int count, int num_sms, int* cta_begin, int* ctas,
+                                      int* order, double* model_ms) {
+  if (!jobs || count < 1 || count > ksvd::kUpdMaxGroups || num_sms < 1 || !cta_begin || !ctas || !order)
+    return KSVD_ERR_INVALID;
+  std::vector<LaneShape> shapes(static_cast<size_t>(count));
+  for (int i = 0; i < count; ++i) {
+    const ksvd_params& p = jobs[i].params;
+    const int64_t N = ksvd_num_patches(&p, jobs[i].width, jobs[i].height);
+    const int n = p.patch_width_dim * p.patch_height_dim;
+    if (N < 1 || n < 1 || p.atoms < 1 || p.omp_iter < 1) return KSVD_ERR_INVALID;
+    const int cap = ksvd::update_res_capacity(n);
+    if (cap < 16) return KSVD_ERR_INVALID;
+    shapes[size_t(i)] = LaneShape{double(N), n, p.atoms, p.omp_iter, cap};
+  }
+  const std::vector<LanePlan> plans = lane_plans(shapes, num_sms);
+  std::vector<int> b, c, o;
+  plan_ranges(plans[0], count, b, c, o);
+  for (int i = 0; i < count; ++i) {
+    cta_begin[i] = b[size_t(i)];
+    ctas[i] = c[size_t(i)];
+    order[i] = o[size_t(i)];
+  }
+  if (model_ms) *model_ms = plans[0].total_ms;
+  return KSVD_OK;
+}
 
 extern "C" ksvd_status ksvd_denoise_many(const ksvd_image_job* jobs, int count, int device, int tune,
                                          ksvd_many_stats* stats) {
@@ -123,8 +256,9 @@ extern "C" ksvd_status ksvd_denoise_many(const ksvd_image_job* jobs, int count, 
 
   MANY_CU(cudaStreamCreateWithFlags(&main_s, cudaStreamNonBlocking));
   for (auto& s : pool) MANY_CU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-  cudaEvent_t t0 = nullptr, t1 = nullptr, t2 = nullptr, t3 = nullptr, ts = nullptr, ti = nullptr;
-  for (cudaEvent_t* e : {&t0, &t1, &t2, &t3, &ts, &ti}) {
+  cudaEvent_t t0 = nullptr, t1 = nullptr, t2 = nullptr, t3 = nullptr, ts = nullptr, ti = nullptr, tm = nullptr,
+              tw = nullptr;
+  for (cudaEvent_t* e : {&t0, &t1, &t2, &t3, &ts, &ti, &tm, &tw}) {
     MANY_CU(cudaEventCreate(e));
     evs.push_back(*e);
   }
@@ -173,12 +307,18 @@ extern "C" ksvd_status ksvd_denoise_many(const ksvd_image_job* jobs, int count, 
     MANY_TRY(ksvd_init_dictionary(j.c, j.d_patches, j.N, j.d_dict));  // synchronises the image's stream
   }
 
-  // ---- the SM split of the shared sweep --------------------------------------
-  std::vector<double> w(static_cast<size_t>(count));
-  for (int i = 0; i < count; ++i)
-    w[size_t(i)] = double(J[size_t(i)].N) * jobs[i].params.omp_iter * (4.0 * J[size_t(i)].n + 8.0);
-  double alpha = 1.0;
-  std::vector<int> ctas = split_ctas(w, alpha, num_sms);
+  // ---- the lane plan of the shared sweep ------------------------------------
+  std::vector<LaneShape> shapes(static_cast<size_t>(count));
+  for (int i = 0; i < count; ++i) {
+    const Job& j = J[size_t(i)];
+    shapes[size_t(i)] = LaneShape{double(j.N), j.n, jobs[i].params.atoms, jobs[i].params.omp_iter,
+                                  ksvd::update_res_capacity(j.n)};
+  }
+  const std::vector<LanePlan> plans = lane_plans(shapes, num_sms);
+  size_t chosen = 0;
+  std::vector<int> cbeg, ctas, order;
+  plan_ranges(plans[0], count, cbeg, ctas, order);
+  std::vector<ksvd::UpdGroup> groups(static_cast<size_t>(count));
 
   ksvd::UpdBatch batch;
   std::memset(&batch, 0, sizeof(batch));
@@ -186,25 +326,26 @@ extern "C" ksvd_status ksvd_denoise_many(const ksvd_image_job* jobs, int count, 
   ksvd_ctx* c0 = J[0].c;
 
   // one batch iteration: fork, per image OMP + atom lists + residual, one
-  // shared sweep on the main stream, join
-  auto iteration = [&](bool omp) -> ksvd_status {
+  // shared sweep on the main stream, join; `mid` (optional) is recorded
+  // between the two
+  auto iteration = [&](bool omp, cudaEvent_t mid) -> ksvd_status {
     cudaEvent_t fk = new_event();
     if (cudaEventRecord(fk, main_s) != cudaSuccess) return KSVD_ERR_CUDA;
     for (auto s : pool)
       if (cudaStreamWaitEvent(s, fk, 0) != cudaSuccess) return KSVD_ERR_CUDA;
-    int begin = 0;
     for (int i = 0; i < count; ++i) {
       Job& j = J[size_t(i)];
       if (omp) KSVD_TRY(omp_form(j.c, j.d_patches, j.N, j.d_dict, j.d_idx, j.d_coef, j.c->p.precision));
-      KSVD_TRY(update_prepare(j.c, j.d_patches, j.N, j.d_dict, j.d_idx, j.d_coef, ctas[size_t(i)], &batch.g[i]));
-      batch.g[i].cta_begin = begin;
-      begin += ctas[size_t(i)];
+      KSVD_TRY(update_prepare(j.c, j.d_patches, j.N, j.d_dict, j.d_idx, j.d_coef, ctas[size_t(i)], &groups[size_t(i)]));
+      groups[size_t(i)].cta_begin = cbeg[size_t(i)];
     }
+    for (int k = 0; k < count; ++k) batch.g[k] = groups[size_t(order[size_t(k)])];  // the sweep's group order
     for (auto s : pool) {
       cudaEvent_t jn = new_event();
       if (cudaEventRecord(jn, s) != cudaSuccess || cudaStreamWaitEvent(main_s, jn, 0) != cudaSuccess)
         return KSVD_ERR_CUDA;
     }
+    if (mid && cudaEventRecord(mid, main_s) != cudaSuccess) return KSVD_ERR_CUDA;
     if (ksvd::launch_update_batch(batch, c0->d_flags, c0->d_stats, 0, num_sms, main_s) != cudaSuccess) {
       cudaGetLastError();
       return KSVD_ERR_CUDA;
@@ -232,9 +373,9 @@ extern "C" ksvd_status ksvd_denoise_many(const ksvd_image_job* jobs, int count, 
         MANY_CU(cudaMemcpyAsync(csave[size_t(i)], j.d_coef, kc * 4, cudaMemcpyDeviceToDevice, j.c->stream));
       }
       double best = 1e300;
-      double best_alpha = 1.0;
-      for (double a : {0.5, 0.75, 1.0}) {
-        ctas = split_ctas(w, a, num_sms);
+      const size_t ntry = std::min<size_t>(plans.size(), 3);
+      for (size_t pi = 0; pi < ntry; ++pi) {
+        plan_ranges(plans[pi], count, cbeg, ctas, order);
         for (int rep = 0; rep < 2; ++rep) {
           for (int i = 0; i < count; ++i) {
             Job& j = J[size_t(i)];
@@ -243,7 +384,7 @@ extern "C" ksvd_status ksvd_denoise_many(const ksvd_image_job* jobs, int count, 
             MANY_CU(cudaMemcpyAsync(j.d_coef, csave[size_t(i)], kc * 4, cudaMemcpyDeviceToDevice, j.c->stream));
           }
           MANY_CU(cudaEventRecord(t2, main_s));
-          MANY_TRY(iteration(false));
+          MANY_TRY(iteration(false, nullptr));
           MANY_CU(cudaEventRecord(t3, main_s));
           MANY_CU(cudaStreamSynchronize(main_s));
           MANY_TRY(check_dev_flags(c0, "batch sweep"));
@@ -251,12 +392,11 @@ extern "C" ksvd_status ksvd_denoise_many(const ksvd_image_job* jobs, int count, 
           cudaEventElapsedTime(&ms, t2, t3);
           if (rep == 1 && ms < best) {
             best = ms;
-            best_alpha = a;
+            chosen = pi;
           }
         }
       }
-      alpha = best_alpha;
-      ctas = split_ctas(w, alpha, num_sms);
+      plan_ranges(plans[chosen], count, cbeg, ctas, order);
       // the first iteration's sweep from the saved state with the chosen split
       for (int i = 0; i < count; ++i) {
         Job& j = J[size_t(i)];
@@ -265,16 +405,17 @@ extern "C" ksvd_status ksvd_denoise_many(const ksvd_image_job* jobs, int count, 
         MANY_CU(cudaMemcpyAsync(j.d_coef, csave[size_t(i)], kc * 4, cudaMemcpyDeviceToDevice, j.c->stream));
       }
       MANY_CU(cudaEventRecord(t1, main_s));  // the timed iterations start here
-      MANY_TRY(iteration(true));
+      MANY_TRY(iteration(true, tm));
     } else {
-      MANY_TRY(iteration(true));  // allocates every workspace buffer
+      MANY_TRY(iteration(true, tm));  // allocates every workspace buffer
     }
+    MANY_CU(cudaEventRecord(tw, main_s));
     if (T > 1) {
       // capture one batch iteration and replay it; if the capture is refused,
       // the iterations run as plain launches
       bool captured = false;
       if (cudaStreamBeginCapture(main_s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
-        const ksvd_status cs = iteration(true);
+        const ksvd_status cs = iteration(true, nullptr);
         const cudaError_t ce = cudaStreamEndCapture(main_s, &graph);
         if (cs == KSVD_OK && ce == cudaSuccess && graph &&
             cudaGraphInstantiate(&gexec, graph, 0) == cudaSuccess)
@@ -291,7 +432,7 @@ extern "C" ksvd_status ksvd_denoise_many(const ksvd_image_job* jobs, int count, 
         if (graph) cudaGraphDestroy(graph);
         gexec = nullptr;
         graph = nullptr;
-        for (int t = 1; t < T; ++t) MANY_TRY(iteration(true));
+        for (int t = 1; t < T; ++t) MANY_TRY(iteration(true, nullptr));
       }
     }
   }
@@ -333,10 +474,20 @@ extern "C" ksvd_status ksvd_denoise_many(const ksvd_image_job* jobs, int count, 
     stats->tune_ms = a;
     cudaEventElapsedTime(&a, ti, t3);
     stats->final_ms = a;
+    if (T > 0) {
+      cudaEventElapsedTime(&a, t1, tm);
+      stats->codes_ms = a;
+      cudaEventElapsedTime(&a, tm, tw);
+      stats->sweep_ms = a;
+    }
     stats->graph = used_graph;
     stats->streams = S;
-    stats->split_alpha = alpha;
-    for (int i = 0; i < count; ++i) stats->update_ctas[i] = ctas[size_t(i)];
+    stats->plan_ms = plans[chosen].total_ms;
+    stats->lanes = int(plans[chosen].width.size());
+    for (int i = 0; i < count; ++i) {
+      stats->update_ctas[i] = ctas[size_t(i)];
+      stats->update_cta_begin[i] = cbeg[size_t(i)];
+    }
   }
   cleanup();
   return KSVD_OK;

@@ -118,16 +118,21 @@ class ManyStats(ctypes.Structure):
         ("total_ms", ctypes.c_double),
         ("graph", ctypes.c_int),
         ("streams", ctypes.c_int),
-        ("split_alpha", ctypes.c_double),
+        ("plan_ms", ctypes.c_double),
         ("update_ctas", ctypes.c_int * 64),
         ("setup_ms", ctypes.c_double),
         ("tune_ms", ctypes.c_double),
         ("final_ms", ctypes.c_double),
+        ("codes_ms", ctypes.c_double),
+        ("sweep_ms", ctypes.c_double),
+        ("lanes", ctypes.c_int),
+        ("update_cta_begin", ctypes.c_int * 64),
     ]
 
     def as_dict(self, count: int) -> dict:
-        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "update_ctas"}
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("update_ctas", "update_cta_begin")}
         d["update_ctas"] = [int(self.update_ctas[i]) for i in range(count)]
+        d["update_cta_begin"] = [int(self.update_cta_begin[i]) for i in range(count)]
         return d
 
 
@@ -245,6 +250,9 @@ def lib():
         L.ksvd_set_update_slice.restype = _int
         L.ksvd_denoise_many.argtypes = [ctypes.POINTER(ImageJob), _int, _int, _int, ctypes.POINTER(ManyStats)]
         L.ksvd_denoise_many.restype = _int
+        L.ksvd_many_plan.argtypes = [ctypes.POINTER(ImageJob), _int, _int, ctypes.POINTER(_int), ctypes.POINTER(_int),
+                                     ctypes.POINTER(_int), ctypes.POINTER(ctypes.c_double)]
+        L.ksvd_many_plan.restype = _int
         _lib = L
     return _lib
 
@@ -491,6 +499,22 @@ def denoise_many(jobs, device: int = 0, tune: bool = True, outs=None):
     if rc != OK:
         raise KsvdError(rc, lib().ksvd_status_string(rc).decode())
     return out_list, st.as_dict(len(jobs))
+
+
+def many_plan(shapes, num_sms: int = 148):
+    """ksvd_many_plan over [(params, width, height), ...] (host only): the
+    shared sweep's lane plan as (cta_begin, ctas, order, modelled ms)."""
+    m = len(shapes)
+    arr = (ImageJob * m)()
+    for i, (params, width, height) in enumerate(shapes):
+        arr[i].params = params
+        arr[i].width, arr[i].height = int(width), int(height)
+    b, c, o = (_int * m)(), (_int * m)(), (_int * m)()
+    ms = ctypes.c_double(0.0)
+    rc = lib().ksvd_many_plan(arr, m, int(num_sms), b, c, o, ctypes.byref(ms))
+    if rc != OK:
+        raise KsvdError(rc, lib().ksvd_status_string(rc).decode())
+    return list(b), list(c), list(o), ms.value
 
 
 def omp_noalloc(params: KsvdParams, patches, dictionary, idx, coef, stream_handle: int | None = None) -> int:

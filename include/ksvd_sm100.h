@@ -260,10 +260,11 @@ ksvd_status ksvd_omp_noalloc(const ksvd_params* p, const float* d_patches, int64
  * (each with its own parameters, noise variance and dictionary) together: per
  * K-SVD iteration the images' OMP, atom lists and residuals run concurrently
  * on a pool of streams and one persistent launch sweeps the atoms of every
- * image at once, the SMs split between the images by their sweep work.  The
- * second and later iterations replay a CUDA graph of the whole batch
- * iteration.  With tune != 0 the split is chosen by timing one sweep per
- * candidate weighting on the first iteration's codes.  The per-image results
+ * image: its CTAs form lanes that run side by side, each lane sweeping its
+ * images one after the other (the plan of ksvd_many_plan).  The second and
+ * later iterations replay a CUDA graph of the whole batch iteration.  With
+ * tune != 0 the three best modelled lane plans are timed on the first
+ * iteration's codes and the fastest is kept.  The per-image results
  * equal ksvd_denoise's for the same parameters.  Every job must have the same
  * ksvd_iter and device, no sub-images and not the learned form.  Replaces the
  * reference's file-by-file loop (batch_denoiser.cpp:36-118, main.cpp:56-112). */
@@ -281,14 +282,25 @@ typedef struct ksvd_many_stats {
   double total_ms;     /* device time of the whole call (uploads to downloads) */
   int graph;           /* 1: iterations 2..T replayed from a CUDA graph */
   int streams;         /* streams in the pool */
-  double split_alpha;  /* SMs split by (sweep bytes)^alpha */
-  int update_ctas[64]; /* CTAs of each image in the shared sweep */
+  double plan_ms;      /* modelled time of the shared sweep's lane plan */
+  int update_ctas[64]; /* CTAs of each image's lane in the shared sweep */
   double setup_ms;     /* uploads, patch gathers, initial dictionaries */
-  double tune_ms;      /* choosing the SM split (0 without tuning) */
+  double tune_ms;      /* choosing the lane plan (0 without tuning) */
   double final_ms;     /* final OMP, rebuild and downloads */
+  double codes_ms;     /* first timed iteration: every image's OMP, atom lists and residual */
+  double sweep_ms;     /* first timed iteration: the shared update sweep */
+  int lanes;           /* CTA lanes of the shared sweep (a lane sweeps its images in turn) */
+  int update_cta_begin[64]; /* first CTA of each image's lane */
 } ksvd_many_stats;
 
 ksvd_status ksvd_denoise_many(const ksvd_image_job* jobs, int count, int device, int tune, ksvd_many_stats* stats);
+
+/* The lane plan of ksvd_denoise_many's shared sweep without tuning, for a GPU
+ * of num_sms SMs (host only, no GPU needed): per image its first CTA and CTA
+ * count (images sharing a range sweep one after the other), the sweep order
+ * of the images (count entries) and the plan's modelled time in ms. */
+ksvd_status ksvd_many_plan(const ksvd_image_job* jobs, int count, int num_sms, int* cta_begin, int* ctas, int* order,
+                           double* model_ms);
 
 /* ---- autotuning -------------------------------------------------------------
  * The update sweep splits each atom's patches over CTAs of about `slice`

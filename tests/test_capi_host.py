@@ -85,3 +85,44 @@ def test_noalloc_rejects_patch_areas_that_do_not_fit_an_int(ksvd, built_lib):
         p = ksvd.make_params(patch_width_dim=pw, patch_height_dim=ph)
         st = built_lib.ksvd_omp_noalloc(ctypes.byref(p), fake, ctypes.c_int64(1000), fake, fake, fake, None)
         assert st == ksvd.ERR_INVALID, (pw, ph, st)
+
+
+def _check_plan(b, c, o, count, sms):
+    # every image once in the order; each image's range inside the grid;
+    # images sharing a range share it exactly (a lane), and lanes are
+    # disjoint and tile the grid
+    assert sorted(o) == list(range(count))
+    lanes = {}
+    for i in range(count):
+        assert c[i] >= 1 and 0 <= b[i] and b[i] + c[i] <= sms
+        lanes.setdefault(b[i], set()).add(c[i])
+    assert all(len(w) == 1 for w in lanes.values())
+    spans = sorted((beg, beg + next(iter(w))) for beg, w in lanes.items())
+    assert spans[0][0] == 0 and spans[-1][1] == sms
+    assert all(spans[k][1] == spans[k + 1][0] for k in range(len(spans) - 1))
+    # the images of a lane are consecutive in the sweep order
+    seen = []
+    for i in o:
+        if not seen or seen[-1] != b[i]:
+            assert b[i] not in seen
+            seen.append(b[i])
+
+
+def test_many_plan_lanes_tile_the_grid(ksvd, built_lib, synth):
+    """ksvd_many_plan (the shared sweep's lane plan, host only) on the uneven
+    64-image workload and on small cases: a valid plan, the small images not
+    given a wide lane of their own, one image alone on every SM."""
+    jobs = synth.many_workload(count=64)
+    shapes = [(ksvd.make_params(patch_width_dim=j["patch"], patch_height_dim=j["patch"], sliding_width=j["stride"],
+                                sliding_height=j["stride"], atoms=256, omp_iter=5), j["side"], j["side"]) for j in jobs]
+    b, c, o, ms = ksvd.many_plan(shapes, 148)
+    _check_plan(b, c, o, 64, 148)
+    assert ms > 0 and len(set(b)) > 1
+    b1, c1, o1, _ = ksvd.many_plan(shapes[:1], 148)
+    assert (b1, c1, o1) == ([0], [148], [0])
+    small = [(ksvd.make_params(patch_width_dim=8, patch_height_dim=8, sliding_width=3, sliding_height=3, atoms=64,
+                               omp_iter=4), 96, 96)] * 5
+    b5, c5, o5, _ = ksvd.many_plan(small, 20)
+    _check_plan(b5, c5, o5, 5, 20)
+    with pytest.raises(ksvd.KsvdError):
+        ksvd.many_plan(shapes[:1], 0)

@@ -43,8 +43,14 @@ def test_denoise_many_vs_oracle_and_single(torch_cuda, ksvd, oracle, synth, tune
     jobs = _jobs(ksvd, synth)
     outs, st = ksvd.denoise_many([(j["params"], j["noisy"], j["sigma2"]) for j in jobs], tune=tune)
     assert st["graph"] == 1, st
-    assert sum(st["update_ctas"]) == torch_cuda.cuda.get_device_properties(0).multi_processor_count
-    assert min(st["update_ctas"]) >= 1
+    # the sweep's lanes: disjoint CTA ranges tiling the grid, every image in one
+    sms = torch_cuda.cuda.get_device_properties(0).multi_processor_count
+    lanes = {}
+    for b, c in zip(st["update_cta_begin"], st["update_ctas"]):
+        assert c >= 1 and 0 <= b and b + c <= sms
+        lanes.setdefault(b, set()).add(c)
+    assert all(len(w) == 1 for w in lanes.values()) and len(lanes) == st["lanes"]
+    assert sum(next(iter(w)) for w in lanes.values()) == sms
     for j, out in zip(jobs, outs):
         p = j["patch"]
         ref, _ = oracle.ksvd_denoise(j["noisy"], j["sigma2"], pw=p, ph=p, sw=j["stride"], sh=j["stride"], atoms=48,
