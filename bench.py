@@ -565,8 +565,11 @@ def main():
         # algorithmic bytes per launch, per patch times the patches of a launch:
         #   omp: read the patch (4n) + write the codes (8L)
         #   update: read the patch once per used atom + code (L(4n+8)) + write coefficients (4L)
+        # (the 16-bit forms' OMP also writes the sweep's residual rows, 4n
+        # more, when no separate residual pass ran)
+        omp_bpp = 4 * n + 8 * L + (4 * n if fam["residual"][0] <= 0.0 else 0)
         if dom == "omp":
-            bytes_per_patch = 4 * n + 8 * L
+            bytes_per_patch = omp_bpp
         else:
             bytes_per_patch = L * (4 * n + 8) + 4 * L
         traffic_file = ROOT / "profiles" / f"traffic_{wl.name}_{args.precision}.json"
@@ -584,7 +587,7 @@ def main():
         # 16-bit forms against the tensor peak, the rest against HBM
         flops_pp = 2 * n * K * L
         per_kernel = {}
-        for f, bpp in (("omp", 4 * n + 8 * L), ("update", L * (4 * n + 8) + 4 * L), ("residual", 8 * n + 8 * L),
+        for f, bpp in (("omp", omp_bpp), ("update", L * (4 * n + 8) + 4 * L), ("residual", 8 * n + 8 * L),
                        ("csr", 12 * L)):
             ms_f = fam[f][0] / max(args.steps, 1)
             if ms_f <= 0:

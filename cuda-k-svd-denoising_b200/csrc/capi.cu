@@ -289,8 +289,9 @@ namespace ksvd {
 namespace api {
 
 ksvd_status omp_form(ksvd_ctx* c, const float* d_patches, int64_t N, const float* d_dict, int32_t* d_idx,
-                     float* d_coef, int precision) {
+                     float* d_coef, int precision, bool for_update) {
   const int n = c->p.patch_width_dim * c->p.patch_height_dim, K = c->p.atoms, L = c->p.omp_iter;
+  c->resid_fused = false;
   double* gram = nullptr;
   KSVD_TRY(wsT(c, "gram", size_t(K) * K, &gram));
   {
@@ -304,10 +305,32 @@ ksvd_status omp_form(ksvd_ctx* c, const float* d_patches, int64_t N, const float
   // <= 256); beyond that, and for the FP32 form, the FP32 kernels run: the
   // resident-dictionary one when it fits, else the streamed one.
   if (precision != KSVD_PREC_FP32 && ksvd::omp_tc_supported(n, K, L)) {
+    // before an update sweep the kernel also writes the sweep's residual rows
+    // (the same buffers and arithmetic as launch_residual)
+    // (patches with fewer than L atoms are listed and formed after it)
+    float* resid = nullptr;
+    int* last = nullptr;
+    int64_t* fix = nullptr;
+    unsigned long long* nfix = nullptr;
+    if (for_update) {
+      KSVD_TRY(wsT(c, "upd_resid", size_t(N) * n, &resid));
+      KSVD_TRY(wsT(c, "upd_last", size_t(N), &last));
+      KSVD_TRY(wsT(c, "omp_fix_list", size_t(N), &fix));
+      KSVD_TRY(wsT(c, "omp_fix_count", 1, &nfix));
+      KSVD_CU(c, cudaMemsetAsync(nfix, 0, sizeof(unsigned long long), c->stream), "fix count");
+    }
     KSVD_CU(c,
             ksvd::launch_omp_tc(d_patches, N, n, d_dict, gram, K, L, d_idx, d_coef, c->num_sms,
-                                precision == KSVD_PREC_FP16_RESCORE ? 1 : 0, c->d_flags, ph, c->stream),
+                                precision == KSVD_PREC_FP16_RESCORE ? 1 : 0, c->d_flags, ph, c->stream, resid, last,
+                                fix, nfix),
             "omp (tensor cores)");
+    if (for_update) {  // timed with the OMP, which formed the other rows
+      KSVD_CU(c,
+              ksvd::launch_residual_list(d_patches, N, n, d_dict, K, L, d_idx, d_coef, resid, last, fix, nfix,
+                                         c->num_sms, c->stream),
+              "residual (listed patches)");
+    }
+    c->resid_fused = for_update;
   } else if (precision != KSVD_PREC_FP32 && ksvd::omp_tcb_supported(n, K, L)) {
     void* scratch = nullptr;
     KSVD_TRY(ws(c, "tcb_scratch", ksvd::omp_tcb_scratch_bytes(n, K), &scratch));
@@ -332,6 +355,12 @@ ksvd_status omp_form(ksvd_ctx* c, const float* d_patches, int64_t N, const float
 static ksvd_status omp_impl(ksvd_ctx* c, const float* d_patches, int64_t N, const float* d_dict, int32_t* d_idx,
                             float* d_coef) {
   return omp_form(c, d_patches, N, d_dict, d_idx, d_coef, c->p.precision);
+}
+
+// The OMP of a K-SVD iteration: an update sweep on the same codes follows.
+static ksvd_status omp_iter_impl(ksvd_ctx* c, const float* d_patches, int64_t N, const float* d_dict, int32_t* d_idx,
+                                 float* d_coef) {
+  return omp_form(c, d_patches, N, d_dict, d_idx, d_coef, c->p.precision, true);
 }
 
 extern "C" {
@@ -370,12 +399,13 @@ ksvd_status update_prepare(ksvd_ctx* c, const float* d_patches, int64_t N, float
     Prof pr(c, "csr", 4);
     KSVD_CU(c, ksvd::launch_csr_build(d_idx, d_coef, N, L, K, w, c->stream), "csr build");
   }
-  {
+  if (!c->resid_fused) {
     Prof pr(c, "residual", 1);
     KSVD_CU(c,
             ksvd::launch_residual(d_patches, N, n, d_dict, K, L, d_idx, d_coef, resid, last, c->num_sms, c->stream),
             "residual");
   }
+  c->resid_fused = false;
   std::memset(g, 0, sizeof(*g));
   g->R = resid;
   g->D = d_dict;
@@ -441,7 +471,7 @@ ksvd_status ksvd_iterate(ksvd_ctx* c, const float* d_patches, int64_t N, float* 
     return fail(c, KSVD_ERR_INVALID, "bad argument");
   KSVD_TRY(check_kernel_support(c));
   for (int i = 0; i < iters; ++i) {
-    KSVD_TRY(omp_impl(c, d_patches, N, d_dict, d_idx, d_coef));
+    KSVD_TRY(omp_iter_impl(c, d_patches, N, d_dict, d_idx, d_coef));
     KSVD_TRY(update_impl(c, d_patches, N, d_dict, d_idx, d_coef));
   }
   return check_dev_flags(c, "kSvd");
@@ -519,7 +549,7 @@ static ksvd_status denoise_image(ksvd_ctx* c, const float* y, int width, int hei
   if (st == KSVD_OK) st = ksvd_init_dictionary(c, d_patches, g.N, d_dict);
   mark(2);
   for (int i = 0; st == KSVD_OK && i < c->p.ksvd_iter; ++i) {
-    st = omp_impl(c, d_patches, g.N, d_dict, d_idx, d_coef);
+    st = omp_iter_impl(c, d_patches, g.N, d_dict, d_idx, d_coef);
     if (st == KSVD_OK) st = update_impl(c, d_patches, g.N, d_dict, d_idx, d_coef);
   }
   mark(3);

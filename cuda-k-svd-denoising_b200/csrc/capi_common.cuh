@@ -125,13 +125,17 @@ inline ksvd_status check_dev_flags(ksvd_ctx* c, const char* where) {
 }
 
 // OMP of the given precision form and one update sweep (capi.cu), the
-// learned proposal's candidates and OMP (proposal.cu).
+// learned proposal's candidates and OMP (proposal.cu).  With for_update, an
+// update sweep on the same codes follows directly: the tensor-core OMP then
+// also writes the sweep's residual rows (c->resid_fused).
 ksvd_status omp_form(ksvd_ctx* c, const float* d_patches, int64_t N, const float* d_dict, int32_t* d_idx,
-                     float* d_coef, int precision);
+                     float* d_coef, int precision, bool for_update = false);
 ksvd_status update_form(ksvd_ctx* c, const float* d_patches, int64_t N, float* d_dict, const int32_t* d_idx,
                         float* d_coef);
 // The CSR and residual of one sweep (on the context's stream) and its group
 // descriptor for launch_update_batch with `ctas` CTAs (cta_begin left 0).
+// The residual is not formed again when the OMP before it wrote it
+// (c->resid_fused, cleared here).
 ksvd_status update_prepare(ksvd_ctx* c, const float* d_patches, int64_t N, float* d_dict, const int32_t* d_idx,
                            float* d_coef, int ctas, ksvd::UpdGroup* g);
 ksvd_status proposal_candidates_impl(ksvd_ctx* c, const float* d_patches, int64_t N, int32_t* d_cand);

@@ -144,7 +144,9 @@ template <bool F16>
 __global__ void __launch_bounds__(kTcThreads, 1)
     omp_tc_kernel(const float* __restrict__ Y, int64_t N, int n, const float* __restrict__ D,
                   const double* __restrict__ Gram, int K, int L, int32_t* __restrict__ idx_out,
-                  float* __restrict__ coef_out, int64_t ntiles, int d_vec4, GridBarrier* flags, DevStats* stats) {
+                  float* __restrict__ coef_out, int64_t ntiles, int d_vec4, float* __restrict__ R_out,
+                  int* __restrict__ last_out, int64_t* __restrict__ fix_list,
+                  unsigned long long* __restrict__ fix_count, int r_vec4, GridBarrier* flags, DevStats* stats) {
   extern __shared__ __align__(128) unsigned char smem[];
   const TcLayout lo = tc_layout(n, K, L);
   unsigned char* Bt = smem + lo.off_b;
@@ -235,9 +237,22 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     }
   };
   int nscored = 0;
+  int64_t p0 = 0;  // first patch of the current tile
+  // chunk kc of patch m's residual row into R_out
+  auto store_row_chunk = [&](int kc, const float (&r)[8]) {
+    float* dst = R_out + (p0 + m) * int64_t(n) + kc * 8;
+    if (r_vec4 && kc * 8 + 8 <= n) {
+      __stcg(reinterpret_cast<float4*>(dst), make_float4(r[0], r[1], r[2], r[3]));
+      __stcg(reinterpret_cast<float4*>(dst) + 1, make_float4(r[4], r[5], r[6], r[7]));
+    } else {
+#pragma unroll
+      for (int e = 0; e < 8; ++e)
+        if (kc * 8 + e < n) __stcg(dst + e, r[e]);
+    }
+  };
 
   for (int64_t tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
-    const int64_t p0 = tile * kTcTile;
+    p0 = tile * kTcTile;
     const int np = (N - p0 < kTcTile) ? int(N - p0) : kTcTile;
     for (int t = tid; t < kTcTile * n; t += kTcThreads) {
       const int p = t / n, k = t - p * n;
@@ -537,10 +552,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       __syncthreads();
       lap(12);
       // ---- residual quarter (FP32), partial norms, next A operand -----------
+      // (with the patch's final coefficients, the row also goes to R_out)
       const bool live = !done && !P.done;
       float nrm = 0.0f, cn = 0.0f;
       if (live) {
         const int cnt = P.cnt;
+        const bool fin = R_out != nullptr && cnt == L;
         const float mean = P.rmean, inv = 1.0f / P.rscale;
         for (int kc = kc_lo; kc < kc_hi; ++kc) {
           float r[8];
@@ -588,6 +605,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 if (kc * 8 + e < n) r[e] = fmaf(-gg, __ldg(dr + e), r[e]);
             }
           }
+          if (fin) store_row_chunk(kc, r);
           unsigned short h[8];
 #pragma unroll
           for (int e = 0; e < 8; ++e) {
@@ -618,12 +636,19 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     __syncthreads();
     if (q == 0 && m < np) {
       const int cnt = P.cnt;
+      int top = -1;  // highest support atom with a nonzero coefficient
       for (int s2 = 0; s2 < L; ++s2) {
         const bool used = s2 < cnt;
         idx_out[(p0 + m) * L + s2] = used ? Ss[m * L + s2] : -1;
         coef_out[(p0 + m) * L + s2] = used ? gam[m * L + s2] : 0.0f;
+        if (used && gam[m * L + s2] != 0.0f) top = max(top, Ss[m * L + s2]);
       }
+      if (last_out) last_out[p0 + m] = top;
     }
+    // patches that stopped before L atoms: their last residual pass ran with
+    // earlier coefficients (or the pursuit ended in the Cholesky step), so
+    // their rows are left to launch_residual over the list
+    if (R_out && q == 0 && m < np && P.cnt < L) fix_list[atomicAdd(fix_count, 1ull)] = p0 + m;
     __syncthreads();
   }
   if (stats && nscored) atomicAdd(&stats->pad, (unsigned long long)nscored);
@@ -642,9 +667,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 size_t omp_tc_smem_bytes(int n, int K, int L) { return tc_layout(n, K, L).total; }
 
 template __global__ void omp_tc_kernel<false>(const float*, int64_t, int, const float*, const double*, int, int,
-                                              int32_t*, float*, int64_t, int, GridBarrier*, DevStats*);
+                                              int32_t*, float*, int64_t, int, float*, int*, int64_t*,
+                                              unsigned long long*, int, GridBarrier*, DevStats*);
 template __global__ void omp_tc_kernel<true>(const float*, int64_t, int, const float*, const double*, int, int,
-                                             int32_t*, float*, int64_t, int, GridBarrier*, DevStats*);
+                                             int32_t*, float*, int64_t, int, float*, int*, int64_t*,
+                                             unsigned long long*, int, GridBarrier*, DevStats*);
 
 bool omp_tc_supported(int n, int K, int L) {
   return L >= 1 && L <= kTcLMax && n >= 1 && K >= 1 && tc_al(K, 16) <= 256 &&
@@ -653,7 +680,8 @@ bool omp_tc_supported(int n, int K, int L) {
 
 cudaError_t launch_omp_tc(const float* patches, int64_t N, int n, const float* dict, const double* gram, int K, int L,
                           int32_t* idx, float* coef, int num_sms, int fp16, GridBarrier* flags, DevStats* stats,
-                          cudaStream_t s) {
+                          cudaStream_t s, float* resid_out, int* last_out, int64_t* fix_list,
+                          unsigned long long* fix_count) {
   const size_t smem = omp_tc_smem_bytes(n, K, L);
   auto kern = fp16 ? omp_tc_kernel<true> : omp_tc_kernel<false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
@@ -661,7 +689,10 @@ cudaError_t launch_omp_tc(const float* patches, int64_t N, int n, const float* d
   const int64_t ntiles = (N + kTcTile - 1) / kTcTile;
   const int grid = int(std::min<int64_t>(ntiles, num_sms));
   const int d_vec4 = ((n & 3) == 0 && (reinterpret_cast<uintptr_t>(dict) & 15) == 0) ? 1 : 0;
-  kern<<<grid, kTcThreads, smem, s>>>(patches, N, n, dict, gram, K, L, idx, coef, ntiles, d_vec4, flags, stats);
+  const int r_vec4 = ((n & 3) == 0 && (reinterpret_cast<uintptr_t>(resid_out) & 15) == 0) ? 1 : 0;
+  if (resid_out && (!last_out || !fix_list || !fix_count)) return cudaErrorInvalidValue;
+  kern<<<grid, kTcThreads, smem, s>>>(patches, N, n, dict, gram, K, L, idx, coef, ntiles, d_vec4, resid_out, last_out,
+                                      fix_list, fix_count, r_vec4, flags, stats);
   return cudaGetLastError();
 }
 

@@ -88,7 +88,8 @@ __host__ __device__ inline int ur_active(int c, int G, int target) {
   return a < G ? a : G;
 }
 
-// residual_kernel: R = Y - X D, one warp per patch.  The patch's atoms and
+// residual_kernel: R = Y - X D, one warp per patch (every patch, or those of
+// a device-side list).  The patch's atoms and
 // coefficients sit in lanes 0..L-1 and are broadcast by shuffles; each lane
 // forms 16-byte pieces of the row with the support atoms' loads in flight
 // together (same FMA order as r = y - sum_s x_s d_s, s ascending).  last[p]
@@ -99,10 +100,18 @@ __global__ void __launch_bounds__(256) residual_kernel(const float* __restrict__
                                                        const float* __restrict__ D, int K, int L,
                                                        const int32_t* __restrict__ idx,
                                                        const float* __restrict__ coef, float* __restrict__ R,
-                                                       int* __restrict__ last, int vec4) {
+                                                       int* __restrict__ last, int vec4,
+                                                       const int64_t* __restrict__ list,
+                                                       const unsigned long long* __restrict__ count) {
   const int lane = threadIdx.x & 31;
   const int64_t warps = int64_t(gridDim.x) * (blockDim.x >> 5);
-  for (int64_t p = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); p < N; p += warps) {
+  int64_t total = N;  // every patch, or list[0 .. *count)
+  if (list) {
+    const unsigned long long c = *count;
+    total = c < static_cast<unsigned long long>(N) ? int64_t(c) : N;
+  }
+  for (int64_t w = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); w < total; w += warps) {
+    const int64_t p = list ? list[w] : w;
     int a = -1;
     float x = 0.0f;
     if (lane < L) {
@@ -272,20 +281,20 @@ __global__ void __launch_bounds__(kUrThreads, 1)
       constexpr int kB = 4;
       for (int t0 = tid; t0 < cnt; t0 += kUrThreads * kB) {
         int e[kB];
-  #pragma unroll
+#pragma unroll
         for (int k = 0; k < kB; ++k) {
           const int t = t0 + k * kUrThreads;
           e[k] = (t < cnt) ? __ldg(entries + beg + sb + t) : 0;
         }
         float x[kB];
         int lt[kB];
-  #pragma unroll
+#pragma unroll
         for (int k = 0; k < kB; ++k) {
           const bool in = t0 + k * kUrThreads < cnt;
           x[k] = in ? __ldcg(coef + e[k]) : 0.0f;
           lt[k] = (in && last != nullptr) ? __ldg(last + e[k] / L) : -1;
         }
-  #pragma unroll
+#pragma unroll
         for (int k = 0; k < kB; ++k) {
           const int t = t0 + k * kUrThreads;
           if (t < cnt) {
@@ -301,7 +310,7 @@ __global__ void __launch_bounds__(kUrThreads, 1)
     auto dot_u = [&](int q) -> float {
       const float4* er = Es4 + size_t(q) * es4;
       float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
-  #pragma unroll 6
+#pragma unroll 6
       for (int f = 0; f < F; ++f) {
         const float4 e = er[f], w = u4[f];
         a0 = fmaf(e.x, w.x, a0);
@@ -409,7 +418,7 @@ __global__ void __launch_bounds__(kUrThreads, 1)
         const float xb = (eb >= 0) ? __ldcg(coef + eb) : 0.0f;
         const float* ra = R + int64_t(ea >= 0 ? ea / L : 0) * n;
         const float* rb = R + int64_t(eb >= 0 ? eb / L : 0) * n;
-  #pragma unroll
+#pragma unroll
         for (int k = 0; k < NW; ++k) {
           const int i = lane + 32 * k;
           e0[k] = (i < n && ea >= 0) ? fmaf(xa, dold[i], __ldcg(ra + i)) : 0.0f;
@@ -425,7 +434,7 @@ __global__ void __launch_bounds__(kUrThreads, 1)
         for (int q = tid; q < mcr; q += kUrThreads) v_s[q] = dot_u(q);
         if (streamed) {  // columns beyond the capacity: a warp per two columns
           float ur[NW], wacc[NW];
-  #pragma unroll
+#pragma unroll
           for (int k = 0; k < NW; ++k) {
             const int i = lane + 32 * k;
             ur[k] = (i < n) ? u[i] : 0.0f;
@@ -436,20 +445,20 @@ __global__ void __launch_bounds__(kUrThreads, 1)
             int ea, eb;
             stream_cols(q, mc, e0, e1, ea, eb);
             float d0 = 0.0f, d1 = 0.0f;
-  #pragma unroll
+#pragma unroll
             for (int k = 0; k < NW; ++k) {
               d0 = fmaf(ur[k], e0[k], d0);
               d1 = fmaf(ur[k], e1[k], d1);
             }
-  #pragma unroll
+#pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
               d0 += __shfl_xor_sync(0xffffffffu, d0, o);
               d1 += __shfl_xor_sync(0xffffffffu, d1, o);
             }
-  #pragma unroll
+#pragma unroll
             for (int k = 0; k < NW; ++k) wacc[k] = fmaf(d1, e1[k], fmaf(d0, e0[k], wacc[k]));
           }
-  #pragma unroll
+#pragma unroll
           for (int k = 0; k < NW; ++k) {
             const int i = lane + 32 * k;
             if (i < n4) wred[(16 + warp) * n4 + i] = wacc[k];
@@ -461,7 +470,7 @@ __global__ void __launch_bounds__(kUrThreads, 1)
           const int f = tid % F, g = tid / F;
           if (g < Gr) {
             float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-  #pragma unroll 4
+#pragma unroll 4
             for (int q = g; q < mcr; q += Gr) {
               const float v = v_s[q];
               const float4 e = Es4[size_t(q) * es4 + f];
@@ -477,7 +486,7 @@ __global__ void __launch_bounds__(kUrThreads, 1)
         float4* gwp = reinterpret_cast<float4*>(gw + (size_t(it & 1) * G + b) * n4);
         for (int f = tid; f < F; f += kUrThreads) {
           float4 acc = wred4[f];
-  #pragma unroll 4
+#pragma unroll 4
           for (int g = 1; g < Gr; ++g) {
             const float4 v = wred4[g * F + f];
             acc.x += v.x;
@@ -486,7 +495,7 @@ __global__ void __launch_bounds__(kUrThreads, 1)
             acc.w += v.w;
           }
           if (streamed)
-  #pragma unroll
+#pragma unroll
             for (int w = 0; w < kUrWarps; ++w) {
               const float4 v = wred4[(16 + w) * F + f];
               acc.x += v.x;
@@ -513,12 +522,12 @@ __global__ void __launch_bounds__(kUrThreads, 1)
             constexpr int kB = 12;  // one round of loads for up to 12 Gr partials per thread
             for (int bb0 = g; bb0 < active; bb0 += Gr * kB) {
               float4 v[kB];
-  #pragma unroll
+#pragma unroll
               for (int k = 0; k < kB; ++k) {
                 const int bb = bb0 + k * Gr;
                 v[k] = (bb < active) ? __ldcg(base + size_t(bb) * F) : make_float4(0.f, 0.f, 0.f, 0.f);
               }
-  #pragma unroll
+#pragma unroll
               for (int k = 0; k < kB; ++k) {
                 acc.x += v[k].x;
                 acc.y += v[k].y;
@@ -537,12 +546,12 @@ __global__ void __launch_bounds__(kUrThreads, 1)
           constexpr int kF = 4;  // float4 per lane (F <= 128)
           float4 wv[kF];
           float s2 = 0.0f;
-  #pragma unroll
+#pragma unroll
           for (int k = 0; k < kF; ++k) {
             const int f = lane + 32 * k;
             float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
             if (f < F)
-  #pragma unroll 4
+#pragma unroll 4
               for (int g = 0; g < Gr; ++g) {
                 const float4 v = wred4[g * F + f];
                 acc.x += v.x;
@@ -560,7 +569,7 @@ __global__ void __launch_bounds__(kUrThreads, 1)
           } else {
             const float inv = 1.0f / sqrtf(nrm2);
             float dm = 0.0f;
-  #pragma unroll
+#pragma unroll
             for (int k = 0; k < kF; ++k) {
               const int f = lane + 32 * k;
               if (f < F) {
@@ -585,7 +594,7 @@ __global__ void __launch_bounds__(kUrThreads, 1)
           }
           if (stop) {
             float sd = 0.0f;
-  #pragma unroll
+#pragma unroll
             for (int k = 0; k < kF; ++k) {
               const int f = lane + 32 * k;
               if (f < F) {
@@ -595,7 +604,7 @@ __global__ void __launch_bounds__(kUrThreads, 1)
             }
             sd = warp_sum(sd);
             if (sd < 0.0f)
-  #pragma unroll
+#pragma unroll
               for (int k = 0; k < kF; ++k) {
                 const int f = lane + 32 * k;
                 if (f < F) {
@@ -630,7 +639,7 @@ __global__ void __launch_bounds__(kUrThreads, 1)
       }
       if (m > cap) {  // streamed columns: a warp per two columns
         float ur[NW];
-  #pragma unroll
+#pragma unroll
         for (int k = 0; k < NW; ++k) {
           const int i = lane + 32 * k;
           ur[k] = (i < n) ? u[i] : 0.0f;
@@ -640,12 +649,12 @@ __global__ void __launch_bounds__(kUrThreads, 1)
           int ea, eb;
           stream_cols(q, m, e0, e1, ea, eb);
           float x0 = 0.0f, x1 = 0.0f;
-  #pragma unroll
+#pragma unroll
           for (int k = 0; k < NW; ++k) {
             x0 = fmaf(ur[k], e0[k], x0);
             x1 = fmaf(ur[k], e1[k], x1);
           }
-  #pragma unroll
+#pragma unroll
           for (int o = 16; o > 0; o >>= 1) {
             x0 += __shfl_xor_sync(0xffffffffu, x0, o);
             x1 += __shfl_xor_sync(0xffffffffu, x1, o);
@@ -654,7 +663,7 @@ __global__ void __launch_bounds__(kUrThreads, 1)
           if (q + kUrWarps >= mc) x1 = 0.0f;
           float* ra = R + int64_t(ea / L) * n;
           if (last == nullptr || __ldg(last + ea / L) != j) {
-  #pragma unroll
+#pragma unroll
             for (int k = 0; k < NW; ++k) {
               const int i = lane + 32 * k;
               if (i < n) __stcg(ra + i, fmaf(-x0, ur[k], e0[k]));
@@ -664,7 +673,7 @@ __global__ void __launch_bounds__(kUrThreads, 1)
           if (eb >= 0) {
             float* rb = R + int64_t(eb / L) * n;
             if (last == nullptr || __ldg(last + eb / L) != j) {
-  #pragma unroll
+#pragma unroll
               for (int k = 0; k < NW; ++k) {
                 const int i = lane + 32 * k;
                 if (i < n) __stcg(rb + i, fmaf(-x1, ur[k], e1[k]));
@@ -761,7 +770,20 @@ cudaError_t launch_residual(const float* Y, int64_t N, int n, const float* D, in
                     (reinterpret_cast<uintptr_t>(D) & 15) == 0 && (reinterpret_cast<uintptr_t>(R) & 15) == 0)
                        ? 1
                        : 0;
-  residual_kernel<<<blocks > 0 ? blocks : 1, 256, 0, s>>>(Y, N, n, D, K, L, idx, coef, R, last, vec4);
+  residual_kernel<<<blocks > 0 ? blocks : 1, 256, 0, s>>>(Y, N, n, D, K, L, idx, coef, R, last, vec4, nullptr,
+                                                          nullptr);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_residual_list(const float* Y, int64_t N, int n, const float* D, int K, int L, const int32_t* idx,
+                                 const float* coef, float* R, int* last, const int64_t* list,
+                                 const unsigned long long* count, int num_sms, cudaStream_t s) {
+  if (!list || !count) return cudaErrorInvalidValue;
+  const int vec4 = ((n & 3) == 0 && (reinterpret_cast<uintptr_t>(Y) & 15) == 0 &&
+                    (reinterpret_cast<uintptr_t>(D) & 15) == 0 && (reinterpret_cast<uintptr_t>(R) & 15) == 0)
+                       ? 1
+                       : 0;
+  residual_kernel<<<num_sms * 2, 256, 0, s>>>(Y, N, n, D, K, L, idx, coef, R, last, vec4, list, count);
   return cudaGetLastError();
 }
 

@@ -84,9 +84,15 @@ cudaError_t launch_omp_stream(const float* patches, int64_t N, int n, const floa
 // OMP with the BF16 tensor-core correlation and exact FP32/FP64 re-scoring.
 size_t omp_tc_smem_bytes(int n, int K, int L);
 bool omp_tc_supported(int n, int K, int L);
+// resid_out (optional, N x n): the residual row y - D_S g of every patch that
+// took L atoms, with its final coefficients, as launch_residual forms it;
+// the others are appended to fix_list (count in *fix_count, zeroed by the
+// caller) for launch_residual's list form.  last_out (with resid_out, N): the
+// highest support atom with a nonzero coefficient (-1 if none).
 cudaError_t launch_omp_tc(const float* patches, int64_t N, int n, const float* dict, const double* gram, int K,
                           int L, int32_t* idx, float* coef, int num_sms, int fp16, GridBarrier* flags,
-                          DevStats* stats, cudaStream_t s);
+                          DevStats* stats, cudaStream_t s, float* resid_out = nullptr, int* last_out = nullptr,
+                          int64_t* fix_list = nullptr, unsigned long long* fix_count = nullptr);
 
 // OMP with the 16-bit tensor-core correlation for dictionaries beyond the
 // resident kernel (atoms <= 512, n <= 256): the 16-bit dictionary streams
@@ -120,6 +126,11 @@ size_t update_res_partial_floats(int n, int grid);
 // last (optional, N ints): the highest atom of each patch's support, -1 if none.
 cudaError_t launch_residual(const float* Y, int64_t N, int n, const float* D, int K, int L, const int32_t* idx,
                             const float* coef, float* R, int* last, int num_sms, cudaStream_t s);
+// The same for the patches list[0 .. *count) only (count read on the device,
+// at most N).
+cudaError_t launch_residual_list(const float* Y, int64_t N, int n, const float* D, int K, int L, const int32_t* idx,
+                                 const float* coef, float* R, int* last, const int64_t* list,
+                                 const unsigned long long* count, int num_sms, cudaStream_t s);
 // sync: 2K unsigned words (zeroed by the launch); gw: update_res_partial_floats.
 // stats receives the counters always, the phase times when timers != 0.
 // One problem of a (multi-problem) update sweep: its buffers (as for
@@ -254,6 +265,9 @@ struct ksvd_ctx {
   std::vector<cudaEvent_t> event_pool;
   int64_t launch_count = 0;
   int upd_slice = 0;  // entries per CTA of the update sweep (0: the kernel's default; ksvd_autotune)
+  // the last OMP (of a K-SVD iteration) already wrote the update's residual
+  // rows and last-atom table; the next update_prepare skips launch_residual
+  bool resid_fused = false;
 
   // Learned support proposal (proposal.cu): shapes, state and the noise
   // variance behind the fallback threshold; its device buffers are named

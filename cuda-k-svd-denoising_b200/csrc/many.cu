@@ -335,7 +335,7 @@ extern "C" ksvd_status ksvd_denoise_many(const ksvd_image_job* jobs, int count, 
       if (cudaStreamWaitEvent(s, fk, 0) != cudaSuccess) return KSVD_ERR_CUDA;
     for (int i = 0; i < count; ++i) {
       Job& j = J[size_t(i)];
-      if (omp) KSVD_TRY(omp_form(j.c, j.d_patches, j.N, j.d_dict, j.d_idx, j.d_coef, j.c->p.precision));
+      if (omp) KSVD_TRY(omp_form(j.c, j.d_patches, j.N, j.d_dict, j.d_idx, j.d_coef, j.c->p.precision, true));
       KSVD_TRY(update_prepare(j.c, j.d_patches, j.N, j.d_dict, j.d_idx, j.d_coef, ctas[size_t(i)], &groups[size_t(i)]));
       groups[size_t(i)].cta_begin = cbeg[size_t(i)];
     }
