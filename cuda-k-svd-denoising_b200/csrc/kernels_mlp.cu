@@ -189,49 +189,76 @@ __global__ void __launch_bounds__(kGThreads) gemm_bf16_kernel(GemmArgs g) {
     const int m = m0 + lg * 32 + lane;
     const unsigned lane_addr = tmem + (unsigned(lg * 32) << 16);
     if (EPI == kEpiTopK) {
-      // warps 0..3: the row's top-k columns (descending score, lower column
-      // first on ties) among the first g.N_valid columns
-      if (warp < 4) {
-        float bv[kMaxTopK];
-        int bi[kMaxTopK];
-        const int kt = g.ktop;
+      // the row's top-k columns (descending score, lower column first on
+      // ties) among the first g.n_valid columns.  The two warps of a TMEM
+      // lane quadrant take one half of the columns each and keep a sorted
+      // list of the 16 best: a new score's place is the number of kept
+      // scores >= it (the columns come in ascending order, so a kept tie is
+      // always the lower column), and the list shifts by predicated moves
+      // without a serial chain.  The halves' lists then meet in shared memory
+      // (the operand stages, free once every MMA has completed) and the
+      // first warp group merges them.
+      const int half = warp >> 2;
+      const int cw = nt / 2;  // a multiple of 8
+      const int ml = lg * 32 + lane;  // row within the tile
+      float bv[kMaxTopK];
+      int bi[kMaxTopK];
 #pragma unroll
-        for (int i = 0; i < kMaxTopK; ++i) {
-          bv[i] = -INFINITY;
-          bi[i] = 0x7fffffff;
-        }
-        for (int c0 = 0; c0 < nt; c0 += 16) {
-          float v[16];
-          tc_ld16(lane_addr + unsigned(c0), v);
-          tc_wait_ld();
+      for (int i = 0; i < kMaxTopK; ++i) {
+        bv[i] = -INFINITY;
+        bi[i] = 0x7fffffff;
+      }
+      for (int c0 = half * cw; c0 < (half + 1) * cw; c0 += 8) {
+        float v[8];
+        tc_ld8(lane_addr + unsigned(c0), v);
+        tc_wait_ld();
 #pragma unroll
-          for (int i = 0; i < 16; ++i) {
-            const int col = n0 + c0 + i;
-            if (col >= g.n_valid) continue;
-            const float z = v[i] + g.bias[col];
-            if (z > bv[kMaxTopK - 1] || (z == bv[kMaxTopK - 1] && col < bi[kMaxTopK - 1])) {
-              // insertion into the sorted list (kMaxTopK entries, only kt used)
-              float cv = z;
-              int ci = col;
+        for (int i = 0; i < 8; ++i) {
+          const int col = n0 + c0 + i;
+          if (col >= g.n_valid) continue;
+          const float z = v[i] + g.bias[col];
+          if (z > bv[kMaxTopK - 1] || (z == bv[kMaxTopK - 1] && col < bi[kMaxTopK - 1])) {
+            int pos = 0;
 #pragma unroll
-              for (int j = 0; j < kMaxTopK; ++j) {
-                const bool better = cv > bv[j] || (cv == bv[j] && ci < bi[j]);
-                if (better) {
-                  const float tv = bv[j];
-                  const int ti = bi[j];
-                  bv[j] = cv;
-                  bi[j] = ci;
-                  cv = tv;
-                  ci = ti;
-                }
+            for (int j = 0; j < kMaxTopK; ++j) pos += (bv[j] >= z) ? 1 : 0;
+#pragma unroll
+            for (int j = kMaxTopK - 1; j >= 0; --j) {
+              if (j > pos) {
+                bv[j] = bv[j - 1 >= 0 ? j - 1 : 0];
+                bi[j] = bi[j - 1 >= 0 ? j - 1 : 0];
+              } else if (j == pos) {
+                bv[j] = z;
+                bi[j] = col;
               }
             }
           }
         }
-        if (m < g.M)
+      }
+      float* zs = reinterpret_cast<float*>(gsm);                 // [2 x 128][16]
+      int* cs = reinterpret_cast<int*>(zs + 2 * kGM * kMaxTopK);  // [2 x 128][16]
+      const int slot = (half * kGM + ml) * kMaxTopK;
 #pragma unroll
-          for (int j = 0; j < kMaxTopK; ++j)
-            if (j < kt) g.topk[(long long)m * kt + j] = bi[j];
+      for (int j = 0; j < kMaxTopK; ++j) {
+        zs[slot + j] = bv[j];
+        cs[slot + j] = bi[j];
+      }
+      __syncthreads();
+      if (half == 0 && m < g.M) {
+        // merge: the first half's columns are the lower ones, so it wins ties
+        const float* za = zs + ml * kMaxTopK;
+        const int* ca = cs + ml * kMaxTopK;
+        const float* zb = zs + (kGM + ml) * kMaxTopK;
+        const int* cb = cs + (kGM + ml) * kMaxTopK;
+        int ia = 0, ib = 0;
+        const int kt = g.ktop;
+        for (int j = 0; j < kt; ++j) {
+          const bool take_a = ib >= kMaxTopK || (ia < kMaxTopK && za[ia] >= zb[ib]);
+          g.topk[(long long)m * kt + j] = take_a ? ca[ia] : cb[ib];
+          if (take_a)
+            ++ia;
+          else
+            ++ib;
+        }
       }
     } else {
       const int half = warp >> 2;  // column half of this warp
