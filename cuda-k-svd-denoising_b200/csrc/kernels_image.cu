@@ -76,15 +76,44 @@ __global__ void __launch_bounds__(256) col2im_kernel(const float* __restrict__ n
       x_l = __ldg(coef + p * L + lane);
       if (a_l < 0 || a_l >= K) a_l = -1;
     }
-    for (int i0 = 0; i0 < g.n; i0 += 32) {
-      const int i = i0 + lane;
-      float v = 0.0f;
-      for (int s = 0; s < L; ++s) {  // L <= 32, the same trip count in every lane
-        const int a = __shfl_sync(0xffffffffu, a_l, s);
-        const float x = __shfl_sync(0xffffffffu, x_l, s);
-        if (a >= 0 && i < g.n) v = fmaf(x, __ldg(D + int64_t(a) * g.n + i), v);
+    // features lane, lane + 32, ... in groups of kCF; per group the rows of
+    // kCS atoms are loaded before their FMAs (sum over s ascending, as in a
+    // plain loop)
+    constexpr int kCF = 5, kCS = 4;
+    for (int i0 = 0; i0 < g.n; i0 += 32 * kCF) {
+      float v[kCF];
+#pragma unroll
+      for (int f = 0; f < kCF; ++f) v[f] = 0.0f;
+      for (int s0 = 0; s0 < L; s0 += kCS) {  // L <= 32, the same trip count in every lane
+        float dv[kCS][kCF];
+        float xv[kCS];
+        bool uv[kCS];
+#pragma unroll
+        for (int u = 0; u < kCS; ++u) {
+          const int s = s0 + u;
+          const int a = __shfl_sync(0xffffffffu, a_l, s & 31);
+          const float x = __shfl_sync(0xffffffffu, x_l, s & 31);
+          const bool use = s < L && a >= 0;
+          uv[u] = use;
+          xv[u] = x;
+#pragma unroll
+          for (int f = 0; f < kCF; ++f) {
+            const int i = i0 + 32 * f + lane;
+            dv[u][f] = (use && i < g.n) ? __ldg(D + int64_t(a) * g.n + i) : 0.0f;
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < kCS; ++u) {
+          if (uv[u])
+#pragma unroll
+            for (int f = 0; f < kCF; ++f) v[f] = fmaf(xv[u], dv[u][f], v[f]);
+        }
       }
-      if (i < g.n) xs[q * g.n + i] = v;
+#pragma unroll
+      for (int f = 0; f < kCF; ++f) {
+        const int i = i0 + 32 * f + lane;
+        if (i < g.n) xs[q * g.n + i] = v[f];
+      }
     }
   }
   __syncthreads();
