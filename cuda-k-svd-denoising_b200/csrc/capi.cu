@@ -339,8 +339,17 @@ ksvd_status omp_form(ksvd_ctx* c, const float* d_patches, int64_t N, const float
                                  precision == KSVD_PREC_FP16_RESCORE ? 1 : 0, scratch, c->d_flags, ph, c->stream),
             "omp (tensor cores, streamed dictionary)");
   } else if (ksvd::omp_fp32_supported(n, K, L)) {
-    KSVD_CU(c, ksvd::launch_omp_fp32(d_patches, N, n, d_dict, gram, K, L, d_idx, d_coef, c->num_sms, ph, c->stream),
+    float* resid = nullptr;
+    int* last = nullptr;
+    if (for_update) {  // the sweep's residual rows from the kernel's own residual tile
+      KSVD_TRY(wsT(c, "upd_resid", size_t(N) * n, &resid));
+      KSVD_TRY(wsT(c, "upd_last", size_t(N), &last));
+    }
+    KSVD_CU(c,
+            ksvd::launch_omp_fp32(d_patches, N, n, d_dict, gram, K, L, d_idx, d_coef, c->num_sms, ph, c->stream,
+                                  resid, last),
             "omp");
+    c->resid_fused = for_update;
   } else {
     KSVD_CU(c,
             ksvd::launch_omp_stream(d_patches, N, n, d_dict, gram, K, L, d_idx, d_coef, c->num_sms, ph, c->stream),

@@ -18,7 +18,8 @@
 //     element per step, only the back substitution runs over the support);
 //   * the residual y - D_S g (:352-380) and its norm (:382-393) are formed
 //     per patch by one warp; a patch whose residual norm is below 1e-3 stops
-//     (:218).
+//     (:218).  Before an update sweep the tile's final residual rows go to
+//     the sweep's residual buffer (the arithmetic of launch_residual).
 #include <cuda_runtime.h>
 
 #include "device_util.cuh"
@@ -87,7 +88,8 @@ __device__ __forceinline__ bool better(float v1, int i1, float v2, int i2) {
 __global__ void __launch_bounds__(kOmpThreads, 1)
     omp_fp32_kernel(const float* __restrict__ Y, int64_t N, int n, const float* __restrict__ D,
                     const double* __restrict__ Gram, int K, int L, int32_t* __restrict__ idx_out,
-                    float* __restrict__ coef_out, int64_t ntiles, DevStats* stats) {
+                    float* __restrict__ coef_out, int64_t ntiles, float* __restrict__ R_out,
+                    int* __restrict__ last_out, DevStats* stats) {
   extern __shared__ __align__(16) unsigned char smem[];
   const OmpLayout lo = omp_layout(n, K, L);
   float* Dk = reinterpret_cast<float*>(smem + lo.off_dk);
@@ -337,6 +339,22 @@ __global__ void __launch_bounds__(kOmpThreads, 1)
       idx_out[(p0 + p) * L + s] = used ? S[p * L + s] : -1;
       coef_out[(p0 + p) * L + s] = used ? gam[p * L + s] : 0.0f;
     }
+    // before an update sweep: the residual rows (Rk holds each patch's
+    // residual with its final coefficients: a patch that stopped kept the
+    // last one formed) and the highest support atom with a nonzero
+    // coefficient
+    if (R_out) {
+      for (int t = tid; t < np * n; t += kOmpThreads) {
+        const int p = t / n, k = t - p * n;
+        __stcg(R_out + (p0 + p) * n + k, Rk[k * rks + p]);
+      }
+      if (tid < np) {
+        int top = -1;
+        for (int s = 0; s < cnt[tid]; ++s)
+          if (gam[tid * L + s] != 0.0f) top = max(top, S[tid * L + s]);
+        last_out[p0 + tid] = top;
+      }
+    }
     __syncthreads();
     lap(10);
   }
@@ -351,13 +369,16 @@ bool omp_fp32_supported(int n, int K, int L) {
 }
 
 cudaError_t launch_omp_fp32(const float* patches, int64_t N, int n, const float* dict, const double* gram, int K,
-                            int L, int32_t* idx, float* coef, int num_sms, DevStats* stats, cudaStream_t s) {
+                            int L, int32_t* idx, float* coef, int num_sms, DevStats* stats, cudaStream_t s,
+                            float* resid_out, int* last_out) {
   size_t smem = omp_fp32_smem_bytes(n, K, L);
   cudaError_t e = cudaFuncSetAttribute(omp_fp32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   int64_t ntiles = (N + kTP - 1) / kTP;
   int grid = int(std::min<int64_t>(ntiles, num_sms));
-  omp_fp32_kernel<<<grid, kOmpThreads, smem, s>>>(patches, N, n, dict, gram, K, L, idx, coef, ntiles, stats);
+  if (resid_out && !last_out) return cudaErrorInvalidValue;
+  omp_fp32_kernel<<<grid, kOmpThreads, smem, s>>>(patches, N, n, dict, gram, K, L, idx, coef, ntiles, resid_out,
+                                                  last_out, stats);
   return cudaGetLastError();
 }
 

@@ -69,11 +69,14 @@ cudaError_t launch_codes_to_dense(const int32_t* idx, const float* coef, int64_t
                                   float* dense, cudaStream_t s);
 
 // OMP (FP32 SIMT correlation).  gram: K x K doubles from launch_gram_f64.
+// resid_out / last_out (optional, together): every patch's residual row with
+// its final coefficients and its highest support atom with a nonzero
+// coefficient, as launch_residual forms them.
 size_t omp_fp32_smem_bytes(int n, int K, int L);
 bool omp_fp32_supported(int n, int K, int L);
 cudaError_t launch_omp_fp32(const float* patches, int64_t N, int n, const float* dict, const double* gram,
                             int K, int L, int32_t* idx, float* coef, int num_sms, DevStats* stats,
-                            cudaStream_t s);
+                            cudaStream_t s, float* resid_out = nullptr, int* last_out = nullptr);
 
 // OMP (FP32 SIMT) with the dictionary streamed through shared memory in
 // feature chunks: any K <= 1024 and n as long as one 4-feature chunk fits.

@@ -363,3 +363,43 @@ def test_build_image_rectangular_vs_oracle(torch_cuda, ksvd, oracle, synth):
     ref, rlam = oracle.build_image(img, 5, 7, 3, 2, D, idx, coef, 400.0, dtype=np.float32)
     assert lam == pytest.approx(rlam, rel=1e-5)
     np.testing.assert_allclose(out.cpu().numpy(), ref, rtol=1e-5, atol=1e-3)
+
+
+@pytest.mark.parametrize("precision", [0, 1, 2])
+def test_fused_residual_matches_separate_pass(torch_cuda, ksvd, synth, precision):
+    """Inside ksvd_iterate the OMP writes the update sweep's residual rows
+    itself (the 16-bit form for patches that took L atoms, the residual
+    kernel forming the rest; the FP32 form from its own residual tile).  The
+    same iteration through ksvd_omp and
+    ksvd_update_dictionary, where the residual kernel forms every row, must
+    give the same dictionary and codes bit for bit.  A zero block makes some
+    patches stop after one atom, so both kinds of rows are exercised."""
+    clean = synth.clean_image(160, 31)
+    noisy = synth.add_gaussian(clean, 20.0, 31).astype(np.float32)
+    noisy[0:36, 0:36] = 0.0  # away from the middle patches that seed the dictionary
+    kw = dict(patch_width_dim=12, patch_height_dim=12, sliding_width=3, sliding_height=3, atoms=128, omp_iter=5,
+              precision=precision, compat=1)
+    c = mkctx(ksvd, **kw)
+    N = ksvd.num_patches(c.params, 160, 160)
+    Y = torch_cuda.empty((N, c.n), dtype=torch_cuda.float32, device="cuda")
+    c.extract_patches(dev(torch_cuda, noisy), Y)
+    D0 = torch_cuda.empty((c.K, c.n), dtype=torch_cuda.float32, device="cuda")
+    c.init_dictionary(Y, D0)
+    out = []
+    for fused in (True, False):
+        D = D0.clone()
+        idx = torch_cuda.empty((N, c.L), dtype=torch_cuda.int32, device="cuda")
+        coef = torch_cuda.empty((N, c.L), dtype=torch_cuda.float32, device="cuda")
+        for _ in range(2):
+            if fused:
+                c.iterate(Y, D, idx, coef, 1)
+            else:
+                c.omp(Y, D, idx, coef)
+                c.update_dictionary(Y, D, idx, coef)
+        torch_cuda.cuda.synchronize()
+        out.append((D.cpu().numpy(), idx.cpu().numpy(), coef.cpu().numpy()))
+    (Df, If, Cf), (Ds, Is, Cs) = out
+    assert np.count_nonzero(If[:, 1] < 0) > 0  # some patches stopped after one atom
+    assert np.array_equal(If, Is)
+    assert np.array_equal(Cf.view(np.uint32), Cs.view(np.uint32))
+    assert np.array_equal(Df.view(np.uint32), Ds.view(np.uint32))
