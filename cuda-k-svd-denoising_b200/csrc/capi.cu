@@ -304,40 +304,47 @@ ksvd_status omp_form(ksvd_ctx* c, const float* d_patches, int64_t N, const float
   // The tensor-core forms need the 16-bit dictionary in shared memory (atoms
   // <= 256); beyond that, and for the FP32 form, the FP32 kernels run: the
   // resident-dictionary one when it fits, else the streamed one.
+  // Before an update sweep the 16-bit kernels also write the sweep's residual
+  // rows (the same buffers and arithmetic as launch_residual); patches that
+  // took fewer than L atoms are listed and formed after them.
+  float* resid = nullptr;
+  int* last = nullptr;
+  int64_t* fix = nullptr;
+  unsigned long long* nfix = nullptr;
+  auto fused_buffers = [&]() -> ksvd_status {
+    KSVD_TRY(wsT(c, "upd_resid", size_t(N) * n, &resid));
+    KSVD_TRY(wsT(c, "upd_last", size_t(N), &last));
+    KSVD_TRY(wsT(c, "omp_fix_list", size_t(N), &fix));
+    KSVD_TRY(wsT(c, "omp_fix_count", 1, &nfix));
+    KSVD_CU(c, cudaMemsetAsync(nfix, 0, sizeof(unsigned long long), c->stream), "fix count");
+    return KSVD_OK;
+  };
+  auto listed_rows = [&]() -> ksvd_status {  // timed with the OMP, which formed the other rows
+    KSVD_CU(c,
+            ksvd::launch_residual_list(d_patches, N, n, d_dict, K, L, d_idx, d_coef, resid, last, fix, nfix,
+                                       c->num_sms, c->stream),
+            "residual (listed patches)");
+    c->resid_fused = true;
+    return KSVD_OK;
+  };
   if (precision != KSVD_PREC_FP32 && ksvd::omp_tc_supported(n, K, L)) {
-    // before an update sweep the kernel also writes the sweep's residual rows
-    // (the same buffers and arithmetic as launch_residual)
-    // (patches with fewer than L atoms are listed and formed after it)
-    float* resid = nullptr;
-    int* last = nullptr;
-    int64_t* fix = nullptr;
-    unsigned long long* nfix = nullptr;
-    if (for_update) {
-      KSVD_TRY(wsT(c, "upd_resid", size_t(N) * n, &resid));
-      KSVD_TRY(wsT(c, "upd_last", size_t(N), &last));
-      KSVD_TRY(wsT(c, "omp_fix_list", size_t(N), &fix));
-      KSVD_TRY(wsT(c, "omp_fix_count", 1, &nfix));
-      KSVD_CU(c, cudaMemsetAsync(nfix, 0, sizeof(unsigned long long), c->stream), "fix count");
-    }
+    if (for_update) KSVD_TRY(fused_buffers());
     KSVD_CU(c,
             ksvd::launch_omp_tc(d_patches, N, n, d_dict, gram, K, L, d_idx, d_coef, c->num_sms,
                                 precision == KSVD_PREC_FP16_RESCORE ? 1 : 0, c->d_flags, ph, c->stream, resid, last,
                                 fix, nfix),
             "omp (tensor cores)");
-    if (for_update) {  // timed with the OMP, which formed the other rows
-      KSVD_CU(c,
-              ksvd::launch_residual_list(d_patches, N, n, d_dict, K, L, d_idx, d_coef, resid, last, fix, nfix,
-                                         c->num_sms, c->stream),
-              "residual (listed patches)");
-    }
-    c->resid_fused = for_update;
+    if (for_update) KSVD_TRY(listed_rows());
   } else if (precision != KSVD_PREC_FP32 && ksvd::omp_tcb_supported(n, K, L)) {
     void* scratch = nullptr;
     KSVD_TRY(ws(c, "tcb_scratch", ksvd::omp_tcb_scratch_bytes(n, K), &scratch));
+    if (for_update) KSVD_TRY(fused_buffers());
     KSVD_CU(c,
             ksvd::launch_omp_tcb(d_patches, N, n, d_dict, gram, K, L, d_idx, d_coef, c->num_sms,
-                                 precision == KSVD_PREC_FP16_RESCORE ? 1 : 0, scratch, c->d_flags, ph, c->stream),
+                                 precision == KSVD_PREC_FP16_RESCORE ? 1 : 0, scratch, c->d_flags, ph, c->stream,
+                                 resid, last, fix, nfix),
             "omp (tensor cores, streamed dictionary)");
+    if (for_update) KSVD_TRY(listed_rows());
   } else if (ksvd::omp_fp32_supported(n, K, L)) {
     float* resid = nullptr;
     int* last = nullptr;

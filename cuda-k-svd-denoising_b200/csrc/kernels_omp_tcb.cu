@@ -163,7 +163,9 @@ __global__ void __launch_bounds__(kTbThreads, 1)
     omp_tcb_kernel(const float* __restrict__ Y, int64_t N, int n, const float* __restrict__ D,
                    const unsigned char* __restrict__ Bg, const float* __restrict__ asum_g,
                    const double* __restrict__ Gram, int K, int L, int32_t* __restrict__ idx_out,
-                   float* __restrict__ coef_out, int64_t ntiles, int d_vec4, GridBarrier* flags, DevStats* stats) {
+                   float* __restrict__ coef_out, int64_t ntiles, int d_vec4, float* __restrict__ R_out,
+                   int* __restrict__ last_out, int64_t* __restrict__ fix_list,
+                   unsigned long long* __restrict__ fix_count, int r_vec4, GridBarrier* flags, DevStats* stats) {
   extern __shared__ __align__(128) unsigned char smem[];
   const TbLayout lo = tb_layout(n, K, L);
   unsigned char* ring = smem + lo.off_ring;
@@ -533,10 +535,12 @@ __global__ void __launch_bounds__(kTbThreads, 1)
       }
       __syncthreads();
       // ---- residual quarter (FP32), partial norms, next A operand -----------
+      // (with the patch's final coefficients, the row also goes to R_out)
       const bool live = !done && !P.done;
       float nrm = 0.0f, cn = 0.0f;
       if (live) {
         const int cnt = P.cnt;
+        const bool fin = R_out != nullptr && cnt == L;
         const float mean = P.rmean, inv = 1.0f / P.rscale;
         for (int kc = kc_lo; kc < kc_hi; ++kc) {
           float r[8];
@@ -572,6 +576,17 @@ __global__ void __launch_bounds__(kTbThreads, 1)
                 if (kc * 8 + e < n) r[e] = fmaf(-gg, __ldg(dr + e), r[e]);
             }
           }
+          if (fin) {
+            float* dst = R_out + (p0 + m) * int64_t(n) + kc * 8;
+            if (r_vec4 && kc * 8 + 8 <= n) {
+              __stcg(reinterpret_cast<float4*>(dst), make_float4(r[0], r[1], r[2], r[3]));
+              __stcg(reinterpret_cast<float4*>(dst) + 1, make_float4(r[4], r[5], r[6], r[7]));
+            } else {
+#pragma unroll
+              for (int e = 0; e < 8; ++e)
+                if (kc * 8 + e < n) __stcg(dst + e, r[e]);
+            }
+          }
           unsigned short h[8];
 #pragma unroll
           for (int e = 0; e < 8; ++e) {
@@ -599,11 +614,17 @@ __global__ void __launch_bounds__(kTbThreads, 1)
     __syncthreads();
     if (q == 0 && m < np) {
       const int cnt = P.cnt;
+      int top = -1;  // highest support atom with a nonzero coefficient
       for (int s2 = 0; s2 < L; ++s2) {
         const bool used = s2 < cnt;
         idx_out[(p0 + m) * L + s2] = used ? Ss[m * L + s2] : -1;
         coef_out[(p0 + m) * L + s2] = used ? gam[m * L + s2] : 0.0f;
+        if (used && gam[m * L + s2] != 0.0f) top = max(top, Ss[m * L + s2]);
       }
+      if (last_out) last_out[p0 + m] = top;
+      // a patch that stopped before L atoms: its rows are left to
+      // launch_residual over the list
+      if (R_out && cnt < L) fix_list[atomicAdd(fix_count, 1ull)] = p0 + m;
     }
     __syncthreads();
   }
@@ -641,8 +662,10 @@ size_t omp_tcb_scratch_bytes(int n, int K) {
 
 cudaError_t launch_omp_tcb(const float* patches, int64_t N, int n, const float* dict, const double* gram, int K,
                            int L, int32_t* idx, float* coef, int num_sms, int fp16, void* scratch,
-                           GridBarrier* flags, DevStats* stats, cudaStream_t s) {
+                           GridBarrier* flags, DevStats* stats, cudaStream_t s, float* resid_out, int* last_out,
+                           int64_t* fix_list, unsigned long long* fix_count) {
   if (!omp_tcb_supported(n, K, L)) return cudaErrorInvalidValue;
+  if (resid_out && (!last_out || !fix_list || !fix_count)) return cudaErrorInvalidValue;
   const TbLayout o = tb_layout(n, K, L);
   unsigned char* Bg = static_cast<unsigned char*>(scratch);
   float* asum = reinterpret_cast<float*>(Bg + size_t(o.Kp) * o.np16 * 2);
@@ -662,8 +685,9 @@ cudaError_t launch_omp_tcb(const float* patches, int64_t N, int n, const float* 
                       (reinterpret_cast<uintptr_t>(patches) & 15) == 0)
                          ? 1
                          : 0;
-  kern<<<grid, kTbThreads, smem, s>>>(patches, N, n, dict, Bg, asum, gram, K, L, idx, coef, ntiles, d_vec4, flags,
-                                      stats);
+  const int r_vec4 = ((n & 3) == 0 && (reinterpret_cast<uintptr_t>(resid_out) & 15) == 0) ? 1 : 0;
+  kern<<<grid, kTbThreads, smem, s>>>(patches, N, n, dict, Bg, asum, gram, K, L, idx, coef, ntiles, d_vec4,
+                                      resid_out, last_out, fix_list, fix_count, r_vec4, flags, stats);
   return cudaGetLastError();
 }
 

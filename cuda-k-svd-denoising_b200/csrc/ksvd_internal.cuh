@@ -102,9 +102,12 @@ cudaError_t launch_omp_tc(const float* patches, int64_t N, int n, const float* d
 // from `scratch` (omp_tcb_scratch_bytes, written by the launch).
 bool omp_tcb_supported(int n, int K, int L);
 size_t omp_tcb_scratch_bytes(int n, int K);
+// resid_out, last_out, fix_list, fix_count (optional): as for launch_omp_tc.
 cudaError_t launch_omp_tcb(const float* patches, int64_t N, int n, const float* dict, const double* gram, int K,
                            int L, int32_t* idx, float* coef, int num_sms, int fp16, void* scratch,
-                           GridBarrier* flags, DevStats* stats, cudaStream_t s);
+                           GridBarrier* flags, DevStats* stats, cudaStream_t s, float* resid_out = nullptr,
+                           int* last_out = nullptr, int64_t* fix_list = nullptr,
+                           unsigned long long* fix_count = nullptr);
 
 // Dictionary update.
 struct CsrWork {

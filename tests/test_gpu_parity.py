@@ -366,18 +366,21 @@ def test_build_image_rectangular_vs_oracle(torch_cuda, ksvd, oracle, synth):
 
 
 @pytest.mark.parametrize("precision", [0, 1, 2])
-def test_fused_residual_matches_separate_pass(torch_cuda, ksvd, synth, precision):
+@pytest.mark.parametrize("shape", [(12, 3, 128), (16, 2, 320)])
+def test_fused_residual_matches_separate_pass(torch_cuda, ksvd, synth, precision, shape):
     """Inside ksvd_iterate the OMP writes the update sweep's residual rows
     itself (the 16-bit form for patches that took L atoms, the residual
-    kernel forming the rest; the FP32 form from its own residual tile).  The
-    same iteration through ksvd_omp and
+    kernel forming the rest; the FP32 form from its own residual tile; 320
+    atoms of 16 x 16 take the streamed-dictionary kernels).  The same
+    iteration through ksvd_omp and
     ksvd_update_dictionary, where the residual kernel forms every row, must
     give the same dictionary and codes bit for bit.  A zero block makes some
     patches stop after one atom, so both kinds of rows are exercised."""
     clean = synth.clean_image(160, 31)
     noisy = synth.add_gaussian(clean, 20.0, 31).astype(np.float32)
     noisy[0:36, 0:36] = 0.0  # away from the middle patches that seed the dictionary
-    kw = dict(patch_width_dim=12, patch_height_dim=12, sliding_width=3, sliding_height=3, atoms=128, omp_iter=5,
+    pw, st, K = shape
+    kw = dict(patch_width_dim=pw, patch_height_dim=pw, sliding_width=st, sliding_height=st, atoms=K, omp_iter=5,
               precision=precision, compat=1)
     c = mkctx(ksvd, **kw)
     N = ksvd.num_patches(c.params, 160, 160)
