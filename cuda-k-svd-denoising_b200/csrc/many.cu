@@ -112,6 +112,36 @@ std::vector<int> even_widths(int total, int k) {
   return w;
 }
 
+// A lane that got no image hands its CTAs to the lane before it (or after
+// it, for the first), so that every CTA sweeps; the lanes' times are then
+// modelled again.
+void absorb_empty_lanes(const std::vector<LaneShape>& sh, LanePlan& p) {
+  size_t l = 0;
+  while (l < p.width.size() && p.width.size() > 1) {
+    if (!p.imgs[l].empty()) {
+      ++l;
+      continue;
+    }
+    if (l > 0) {
+      p.width[l - 1] += p.width[l];
+    } else {
+      p.width[1] += p.width[0];
+      p.begin[1] = p.begin[0];
+    }
+    p.begin.erase(p.begin.begin() + long(l));
+    p.width.erase(p.width.begin() + long(l));
+    p.imgs.erase(p.imgs.begin() + long(l));
+    p.ms.erase(p.ms.begin() + long(l));
+  }
+  p.total_ms = 0.0;
+  for (size_t k = 0; k < p.width.size(); ++k) {
+    double t = 0.0;
+    for (int i : p.imgs[k]) t += sweep_model_ms(sh[size_t(i)], p.width[k]);
+    p.ms[k] = t;
+    p.total_ms = std::max(p.total_ms, t);
+  }
+}
+
 // Candidate lane plans for the shared sweep, best modelled first:
 //  * k equal lanes, images assigned longest first;
 //  * one wide lane of W CTAs running the nb images that take longest there,
@@ -146,6 +176,7 @@ std::vector<LanePlan> lane_plans(const std::vector<LaneShape>& sh, int G) {
       }
     }
   }
+  for (LanePlan& p : out) absorb_empty_lanes(sh, p);
   std::stable_sort(out.begin(), out.end(), [](const LanePlan& x, const LanePlan& y) { return x.total_ms < y.total_ms; });
   return out;
 }

@@ -3,6 +3,8 @@ symbol, and its host-only entry points behave (no GPU work)."""
 
 import ctypes
 
+import numpy as np
+
 import pytest
 
 
@@ -124,5 +126,13 @@ def test_many_plan_lanes_tile_the_grid(ksvd, built_lib, synth):
                                omp_iter=4), 96, 96)] * 5
     b5, c5, o5, _ = ksvd.many_plan(small, 20)
     _check_plan(b5, c5, o5, 5, 20)
+    # subsets of every size: every lane gets an image (an empty lane hands
+    # its CTAs to a neighbour), so the lanes always tile the grid
+    rng = np.random.default_rng(7)
+    for m in (2, 3, 5, 9, 17, 33):
+        sub = [shapes[i] for i in rng.choice(64, size=m, replace=False)]
+        bs, cs, os_, ms_s = ksvd.many_plan(sub, 148)
+        _check_plan(bs, cs, os_, m, 148)
+        assert ms_s > 0
     with pytest.raises(ksvd.KsvdError):
         ksvd.many_plan(shapes[:1], 0)
