@@ -161,7 +161,8 @@ struct UpdBatch {
 };
 int update_res_capacity(int n);
 // One cooperative launch of `grid` CTAs (one per SM at most) over all groups;
-// the groups' CTA ranges must tile [0, grid) in order.
+// each group's CTA range lies in [0, grid); groups whose ranges share CTAs run
+// one after the other on them, in table order.
 cudaError_t launch_update_batch(const UpdBatch& batch, GridBarrier* flags, DevStats* stats, int timers, int grid,
                                 cudaStream_t s);
 // last (optional): from launch_residual; a residual row is not stored back by
