@@ -391,7 +391,7 @@ extern "C" ksvd_status ksvd_denoise_many(const ksvd_image_job* jobs, int count, 
   int used_graph = 0;
   if (T > 0) {
     if (tune) {
-      // codes of the first iteration, then one timed sweep per weighting,
+      // codes of the first iteration, then one timed sweep per lane plan,
       // each from saved copies of the dictionaries and coefficients
       std::vector<float*> dsave(static_cast<size_t>(count)), csave(static_cast<size_t>(count));
       for (int i = 0; i < count; ++i) {
